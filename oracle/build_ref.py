@@ -1,0 +1,189 @@
+#!/usr/bin/env python3
+"""Build recipe for the reference oracle (test infrastructure only).
+
+Compiles the reference HARM sources *where they lie* (read from the reference
+tree given by ``--src``) into a shared library under ``oracle/_ref/``.  The
+sources are copied to a scratch build directory inside ``oracle/_ref/build/``,
+a fixed list of build patches is applied there (never to the reference tree),
+and the result is linked together with ``oracle/ref_harness.c`` (the probe API
+the tests call through ctypes).  Nothing produced here is committed
+(``oracle/_ref/`` is git-ignored) and nothing here is shipped by the product.
+
+Grid size (N1, N2), the physics mode and the metric are compile-time constants
+in the reference (global.h:126-127, global.h:202, metric.h:11), so each
+problem/size pair is its own library: ``libharmref_<problem>_<N1>x<N2>.so``.
+
+Build patches (each one asserted to apply exactly):
+  1. mympi.h:15          USEMPI 1 -> 0            (no MPI here; serial oracle)
+  2. global.h:202        EOMTYPE per problem      (EOMGRMHD for the torus)
+  3. metric.h:11         MCOORD per problem       (KSCOORDS for the torus)
+  4. global.h:126-127    N1, N2 per build
+  5. torus: init.fishmon.c -> init.c, bounds.fishmon.c -> bounds.c
+  6. gcc >= 10 needs -fcommon (tentative definitions in defs.h)
+  7. dudp_calc.c, utoprim_{1d,2d,5d2}_final.c are left out (gcc rejects their
+     block-scope static prototypes); they are only reached through the
+     UTOPRIMTRYAGAIN chain, which patch 10 disables, so ref_harness.c gives
+     them stubs that fail loudly if ever called.
+  8. init_postfield() and cot() shims (init.fishmon.c predates the former,
+     metric.c:1444 comments out the latter) live in ref_harness.c.
+  9. init_mpi.c:2341-2418 logging: va_copy before every vfprintf (the
+     reference re-uses one va_list, which is undefined behaviour and crashed).
+ 10. global.h:213 UTOPRIMTRYAGAIN 1 -> 0, global.h:34 MAILWHENDONE 1 -> 0,
+     global.h:24 PRODUCTION 0 -> 1 (progress printing only).
+ 11. utoprim_2d.c:669 the Newton cycle-break factor rand()/RAND_MAX is
+     replaced by hr_cycle_break_uniform(x[0], x[1], n_iter), a counter-based
+     hash of the iterate (same function as the GPU kernel and the C
+     restatement use), so that the factor no longer depends on a serial
+     global RNG stream.
+ 12. init.fishmon.c init_grid()/init_global() and dump.c dump() are renamed;
+     ref_harness.c wraps the first two to apply the benchmark knobs
+     (defcoord 0, Rin = 0.98 r_h, MC/PARA, HLL/LAXF, RK2, courant, floors)
+     and turns dump files off.
+ 13. compiled -O2 -ffp-contract=off -fno-fast-math so that no FMA
+     contraction changes the FP64 rounding.
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import re
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+
+# reference file list of the default build (maketail.harm.inc:1-9), minus main.c
+# (the harness is the driver) and the four files of patch 7.
+BASE_SRCS = """bounds.c boundsint.c coord.c diag.c dudp_calc_3vel.c dump.c dump_ener.c
+fixup.c gaussj.c image.c initbase.c init.c interp.c lubksb.c ludcmp.c metric.c mnewt.c
+nrutil.c phys.c ranc.c restart.c set_arrays.c set_grid.c step_ch.c tensor.c utoprim.c
+utoprim_2d.c utoprim_1d.c utoprim_1d_opt.c vchar.c transforms.c fail.c utoprim_ldz.c
+init_mpi.c boundmpi.c boundmpiint.c sources.c phys.ffde.c advance.c reconstructeno.c""".split()
+
+PROBLEMS = {
+    # Fishbone-Moncrief torus in modified Kerr-Schild coordinates (GRMHD).
+    "torus": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c"),
+}
+
+CFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-fPIC", "-w", "-std=gnu99"]
+
+
+def sub1(text, pattern, repl, fname, count=1, regex=False):
+    """Replace exactly `count` occurrences, failing loudly otherwise."""
+    if regex:
+        new, n = re.subn(pattern, repl, text)
+    else:
+        n = text.count(pattern)
+        new = text.replace(pattern, repl)
+    if n != count:
+        raise SystemExit(f"patch failed in {fname}: expected {count} match(es) of {pattern!r}, got {n}")
+    return new
+
+
+def patch_tree(bdir, problem, n1, n2):
+    prob = PROBLEMS[problem]
+
+    def edit(fname, fn):
+        path = os.path.join(bdir, fname)
+        with open(path, "r", encoding="latin-1") as f:
+            txt = f.read()
+        txt = fn(txt, fname)
+        with open(path, "w", encoding="latin-1") as f:
+            f.write(txt)
+
+    edit("mympi.h", lambda t, f: sub1(t, "#define USEMPI 1", "#define USEMPI 0", f))
+
+    def g(t, f):
+        t = sub1(t, r"#define N1\s+64", f"#define N1 {n1}", f, regex=True)
+        t = sub1(t, r"#define N2\s+64", f"#define N2 {n2}", f, regex=True)
+        t = sub1(t, "#define EOMTYPE EOMFFDE", f"#define EOMTYPE {prob['eom']}", f)
+        t = sub1(t, "#define UTOPRIMTRYAGAIN 1", "#define UTOPRIMTRYAGAIN 0", f)
+        t = sub1(t, "#define MAILWHENDONE 1", "#define MAILWHENDONE 0", f)
+        t = sub1(t, "#define PRODUCTION 0", "#define PRODUCTION 1", f)
+        return t
+    edit("global.h", g)
+    edit("metric.h", lambda t, f: sub1(t, "#define MCOORD CYLMINKMETRIC", f"#define MCOORD {prob['mcoord']}", f))
+
+    shutil.copyfile(os.path.join(bdir, prob["init"]), os.path.join(bdir, "init.c"))
+    shutil.copyfile(os.path.join(bdir, prob["bounds"]), os.path.join(bdir, "bounds.c"))
+
+    def ini(t, f):
+        t = sub1(t, "int init_grid(void)", "int hr_orig_init_grid(void)", f)
+        t = sub1(t, "int init_global(void)", "int hr_orig_init_global(void)", f)
+        return t
+    edit("init.c", ini)
+    edit("dump.c", lambda t, f: sub1(t, "int dump(long dump_cnt)\n", "int hr_orig_dump(long dump_cnt)\n", f))
+
+    def logfix(t, f):
+        # every vfprintf(X, format, arglist) consumes a private copy of the list
+        return sub1(t, r"vfprintf \((\w+), format, arglist\);",
+                    r"{ va_list hr_ac; va_copy(hr_ac, arglist); vfprintf (\1, format, hr_ac); va_end(hr_ac); }",
+                    f, count=8, regex=True)
+    edit("init_mpi.c", logfix)
+
+    def u2d(t, f):
+        t = sub1(t, "randtmp = ( (1.*rand())/(1.*RAND_MAX) );",
+                 "randtmp = hr_cycle_break_uniform(x[0], x[1], n_iter);", f)
+        t = sub1(t, '#include "utoprim_2d.h"',
+                 '#include "utoprim_2d.h"\nextern FTYPE hr_cycle_break_uniform(FTYPE x0, FTYPE x1, int n_iter);', f)
+        return t
+    edit("utoprim_2d.c", u2d)
+
+
+def build(src, problem, n1, n2, jobs, force=False):
+    tag = f"{problem}_{n1}x{n2}"
+    lib = os.path.join(OUT, f"libharmref_{tag}.so")
+    harness = os.path.join(HERE, "ref_harness.c")
+    if (not force and os.path.exists(lib)
+            and os.path.getmtime(lib) >= os.path.getmtime(harness)
+            and os.path.getmtime(lib) >= os.path.getmtime(__file__)):
+        return lib
+    bdir = os.path.join(OUT, "build", tag)
+    if os.path.isdir(bdir):
+        shutil.rmtree(bdir)
+    os.makedirs(bdir)
+    for name in os.listdir(src):
+        if name.endswith((".c", ".h")):
+            shutil.copyfile(os.path.join(src, name), os.path.join(bdir, name))
+    patch_tree(bdir, problem, n1, n2)
+    shutil.copyfile(harness, os.path.join(bdir, "hr_harness.c"))
+    srcs = BASE_SRCS + ["hr_harness.c"]
+
+    def cc(name):
+        obj = os.path.join(bdir, name[:-2] + ".o")
+        cmd = ["gcc"] + CFLAGS + ["-c", os.path.join(bdir, name), "-o", obj]
+        r = subprocess.run(cmd, cwd=bdir, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"compile failed: {name}\n{r.stderr[-3000:]}")
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(cc, srcs))
+    tmp = lib + ".tmp"
+    r = subprocess.run(["gcc", "-shared", "-Wl,-Bsymbolic", "-o", tmp] + objs + ["-lm"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed\n" + r.stderr[-3000:])
+    os.replace(tmp, lib)
+    return lib
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--problem", default="torus", choices=sorted(PROBLEMS))
+    ap.add_argument("--sizes", default="16x16,32x32,64x64,128x128")
+    ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    if not os.path.isdir(a.src):
+        print(f"reference tree {a.src} not present; nothing built", file=sys.stderr)
+        return 0
+    for s in a.sizes.split(","):
+        n1, n2 = (int(v) for v in s.split("x"))
+        print(build(a.src, a.problem, n1, n2, a.jobs, a.force))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
