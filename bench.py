@@ -1,0 +1,327 @@
+#!/usr/bin/env python3
+"""Throughput of HARM's per-step update on B200: zone-cycles/s on the 512^2
+Fishbone-Moncrief torus (FP64, PPM reconstruction, HLL flux, flux-CT, 2D
+Newton con-to-prim, midpoint RK2).  One zone-cycle = one active zone advanced
+by one full RK2 step (the reference's nstep convention, main.c:54,88).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+The b200 arm runs the CUDA step (device-resident state, CUDA graph per step);
+under torchrun each rank advances its own torus (replicas only: the path has
+no exchange step on one GPU) and the value is the aggregate over ranks timed
+as the maximum over ranks.  The reference arm times the reference's own CPU
+step (compiled from its sources into oracle/_ref) on the host cores, one
+process per core, each on its own torus.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "zone-cycles/s, 512² torus"
+UNIT = "zone-cycles/s"
+BYTES_PER_ZONE_CYCLE = 2032  # algorithmic FP64 bytes per zone-cycle
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--lim", default="para", choices=["para", "mc"])
+    ap.add_argument("--flux", default="hll", choices=["hll", "laxf"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) > 8:
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ reference
+def _ref_lib(n):
+    p = os.path.join(ROOT, "oracle", "_ref", f"libharmref_torus_{n}x{n}.so")
+    return p if os.path.exists(p) else None
+
+
+REF_WORKER = r"""
+import ctypes, os, sys, time, tempfile
+lib = ctypes.CDLL(sys.argv[1])
+lim, nsteps = int(sys.argv[2]), int(sys.argv[3])
+lib.hr_configure.argtypes = [ctypes.c_int]*3 + [ctypes.c_double, ctypes.c_int, ctypes.c_double]
+lib.hr_configure(lim, int(sys.argv[4]), 2, 0.8, 0, 1e30)
+w = tempfile.mkdtemp(prefix="harmref_")
+fd = os.open(os.devnull, os.O_WRONLY); sv = os.dup(1); os.dup2(fd, 1); os.dup2(fd, 2)
+lib.hr_init(w.encode())
+ts = []
+for k in range(nsteps):
+    t0 = time.perf_counter(); rc = lib.hr_step(1); ts.append(time.perf_counter() - t0)
+    if rc: break
+os.write(sv, (" ".join("%.6f" % t for t in ts) + "\n").encode())
+"""
+
+
+def run_reference_procs(n, lim, flux, nsteps, nprocs):
+    """nprocs independent reference processes (one torus each); per-step wall
+    times of each.  Returns a list of lists."""
+    lib = _ref_lib(n)
+    if lib is None:
+        return None
+    procs = [subprocess.Popen([sys.executable, "-c", REF_WORKER, lib, str(lim), str(nsteps), str(flux)],
+                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL) for _ in range(nprocs)]
+    out = []
+    for p in procs:
+        so, _ = p.communicate()
+        line = so.decode().strip().splitlines()
+        out.append([float(x) for x in line[-1].split()] if line else [])
+    return out
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = a.n
+    lim = 4 if a.lim == "para" else 3
+    flux = 1 if a.flux == "hll" else 0
+    cfg = {"workload": f"{n}x{n} Fishbone-Moncrief torus, MKS a=0.9375, FP64, {a.lim.upper()} + {a.flux.upper()}, "
+                       "flux-CT, 2D Newton con-to-prim, RK2 midpoint, courant 0.8", "n1": n, "n2": n,
+           "parallelism": "one process per host core, independent tori"}
+    if _ref_lib(n) is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libharmref_torus_%dx%d.so "
+                                                              "not present (built from the reference sources by "
+                                                              "__graft_entry__.build())" % (n, n)}))
+        return 0
+    nprocs = max(1, min(cpu_cores(), 16))
+    t0 = time.time()
+    per = run_reference_procs(n, lim, flux, a.warmup + a.steps, nprocs)
+    per = [p for p in per if len(p) == a.warmup + a.steps]
+    if not per:
+        print(json.dumps({"impl": "reference", "unavailable": "reference step failed"}))
+        return 0
+    # aggregate: all processes advance concurrently; a timed step is the
+    # slowest process's step
+    step_times = [max(p[a.warmup + k] for p in per) for k in range(a.steps)]
+    tstep = sum(step_times) / len(step_times)
+    value = len(per) * n * n / tstep
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": tstep * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded torus of the reference's own init)", "config": cfg,
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(per), "kind": "reference",
+                             "sample": f"{len(per)} processes x ({a.warmup} warm-up + {a.steps} timed) reference "
+                                       f"steps of a {n}x{n} torus after init; wall {time.time() - t0:.0f}s"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ b200 arm
+def b200_arm(a):
+    import torch
+    import harm_ramt_b200 as hb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    n = a.n
+    lim = hb.LIM_PARA if a.lim == "para" else hb.LIM_MC
+    flux = hb.FLUX_HLL if a.flux == "hll" else hb.FLUX_LAXF
+    h, geom, p0 = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (also instantiates the CUDA graph of one step)
+    h.step_ch(a.warmup)
+    h.sync()
+    # per-kernel device times of one step, events after every launch
+    prof = h.profile_step()
+    h.sync()
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    h.step_ch(a.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    st = h.sync()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / a.steps
+    value = world * n * n / (ms_step * 1e-3)
+
+    # end to end through the C ABI with host buffers: each step uploads the
+    # state from host memory, advances it and reads it back
+    host_p, _ = h.get_prims()
+    h2d = host_p.nbytes
+    d2h = host_p.nbytes + host_p.shape[0] * host_p.shape[1] * 5 * 4
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.e2e_steps):
+        h.set_prims(host_p, reset_gammacheck=False)
+        h.step_ch(1)
+        host_p, host_f = h.get_prims()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / a.e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * n * n / e2e_s
+
+    # roofline of the dominant kernel (largest share of the step's device time)
+    peak, peak_kind = peaks()
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_launches = prof[dom]
+    per_launch_ms = dom_ms / max(dom_launches, 1)
+    alg_bytes = KERNEL_BYTES.get(dom, 0) * n * n
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    step_alg = BYTES_PER_ZONE_CYCLE * n * n / (ms_step * 1e-3) / 1e9
+    total_prof = sum(v[0] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRAFFIC.get(dom),
+                "bytes_per_zone": KERNEL_BYTES.get(dom, 0), "launch_ms": per_launch_ms,
+                "share_of_step": dom_ms / total_prof if total_prof else None,
+                "whole_step": {"achieved": step_alg, "frac": step_alg / peak,
+                               "bytes_per_zone_cycle": BYTES_PER_ZONE_CYCLE},
+                "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()}}
+
+    launches = sum(v[1] for v in prof.values()) * a.steps
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        per = run_reference_procs(n, 4 if a.lim == "para" else 3, 1 if a.flux == "hll" else 0, 2, 1)
+        if per and len(per[0]) == 2:
+            t1 = per[0][1]
+            cpu = {"value": n * n / t1, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"reference step_ch() of the {n}x{n} torus on one host core, second step after init "
+                             f"({t1:.2f} s)"}
+    h.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Fishbone-Moncrief torus, init of "
+                                                             "init.fishmon.c restated on the host)",
+                "config": {"workload": f"{n}x{n} Fishbone-Moncrief torus, MKS a=0.9375, FP64, "
+                                       f"{a.lim.upper()} + {a.flux.upper()}, flux-CT, 2D Newton con-to-prim, "
+                                       "RK2 midpoint, courant 0.8", "n1": n, "n2": n,
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": "working set per step (geometry 126 planes x %.1f MB) exceeds L2" %
+                                 ((n + 6) * (n + 6) * 8 / 1e6)},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.warmup + a.steps + 1) * 2 * n * n),
+                "t_end": st["t"], "dt_end": st["dt"]}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+# algorithmic bytes per active zone of one launch (FP64)
+KERNEL_BYTES = {
+    "k_flux": 8 * (8 + 2 * 21 + 2 * 8),       # prims once, FACE1+FACE2 geometry, F1+F2 out
+    "k_update": 8 * (8 + 8 + 21 + 40 + 2 + 2 * 8 + 1 + 8) + 4,  # pi, pb, CENT geo, conn, floors, 2 faces x2, emf, pf, pflag
+    "k_emf": 8 * (2 + 5 + 1),
+    "k_bsqflags": 8 * (8 + 21) + 1,
+}
+TRAFFIC = {}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return reference_arm(a)
+    return b200_arm(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,270 @@
+"""B200 (sm_100a) implementation of HARM's per-step finite-volume update.
+
+Python host mirror of the C ABI in include/harm_b200.h (loaded with ctypes
+from the in-tree libharm_b200.so).  The operator is the reference's
+``step_ch()`` (step_ch.c:16): :class:`HarmGPU` holds the device-resident copy
+of the reference globals it reads and writes (p, pflag, t, dt and the
+geometry tables) and :meth:`HarmGPU.step_ch` advances them by whole steps.
+
+Arrays use the reference's layout (defs.h) over the full grid including the
+3 ghost zones on each side: prims ``[n1+6, n2+6, 8]``, pflag
+``[n1+6, n2+6, 5]``, gcov/gcon ``[n1+6, n2+6, 4, 4, 4]``, gdet
+``[n1+6, n2+6, 4]``, conn ``[n1+6, n2+6, 4, 4, 4]``, floors
+``[n1+6, n2+6, 2]``.
+
+There is no CPU fallback: the step runs only on the CUDA device and fails
+loudly when the library or the device is missing.  The torus set-up helpers
+(:func:`torus_geometry`, :func:`torus_init`) are host code of the plugin
+surface and run anywhere.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["HarmGPU", "HarmError", "torus_params", "torus_geometry", "torus_init", "load_library", "LIB_PATH",
+           "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "NG", "NPR"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libharm_b200.so")
+NG = 3
+NPR = 8
+LIM_MC, LIM_PARA = 3, 4
+FLUX_LAXF, FLUX_HLL = 0, 1
+
+_ERRORS = {0: "ok", 1: "invalid argument", 2: "no usable CUDA device (sm_100 required)", 3: "CUDA runtime error",
+           4: "device allocation failed", 5: "geometry tables missing or not symmetric",
+           6: "fatal check of the reference step fired"}
+# fail() codes of the reference, global.h:562-579
+FAIL_NAMES = {1: "UTOPRIM_NEG", 2: "UTOPRIM_TEST", 3: "VCHAR_DISCR", 4: "COEFF_NEG", 5: "COEFF_SUP",
+              6: "UTCALC_DISCR", 7: "FAIL_LDZ", 8: "FAIL_BCFIX", 9: "FAIL_VSQ_NEG"}
+
+
+class HarmError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: {_ERRORS.get(code, 'error %d' % code)}" if what else _ERRORS.get(code, str(code)))
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("lim", ctypes.c_int), ("fluxmethod", ctypes.c_int),
+                ("eom", ctypes.c_int), ("reserved", ctypes.c_int), ("cour", ctypes.c_double),
+                ("gam", ctypes.c_double), ("dx1", ctypes.c_double), ("dx2", ctypes.c_double),
+                ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
+                ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
+                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double)]
+
+
+class _Status(ctypes.Structure):
+    _fields_ = [("fail_code", ctypes.c_int), ("fail_i", ctypes.c_int), ("fail_j", ctypes.c_int),
+                ("fixups", ctypes.c_int), ("realnstep", ctypes.c_longlong), ("t", ctypes.c_double),
+                ("dt", ctypes.c_double), ("newton_iters", ctypes.c_ulonglong)]
+
+
+class _TorusParams(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("seed", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("a", ctypes.c_double), ("hslope", ctypes.c_double), ("rout", ctypes.c_double),
+                ("rin_over_rhor", ctypes.c_double), ("gam", ctypes.c_double), ("torus_rin", ctypes.c_double),
+                ("torus_rmax", ctypes.c_double), ("kappa", ctypes.c_double), ("beta", ctypes.c_double),
+                ("randfact", ctypes.c_double), ("rhomin", ctypes.c_double), ("uumin", ctypes.c_double),
+                ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double), ("gammamax", ctypes.c_double)]
+
+
+_lib = None
+
+EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
+           "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
+           "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
+           "harm_kernel_name"]
+
+
+def load_library(path=None):
+    """Loads libharm_b200.so (building it first when nvcc is available and
+    the sources are newer).  Raises if the library cannot be loaded."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if path is None:
+        try:
+            from . import build as _build
+            if _build.needs_build():
+                _build.build()
+        except Exception as e:  # a prebuilt library is still usable
+            if not os.path.exists(p):
+                raise RuntimeError(f"libharm_b200.so is missing and could not be built: {e}") from e
+    lib = ctypes.CDLL(p)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    lib.harm_create.argtypes = [ctypes.POINTER(_Config), vp, ctypes.POINTER(vp)]
+    lib.harm_upload_geometry.argtypes = [vp, dp, dp, dp, dp, dp]
+    lib.harm_set_prims.argtypes = [vp, dp, ip, ctypes.c_int]
+    lib.harm_get_prims.argtypes = [vp, dp, ip]
+    lib.harm_bound_prims.argtypes = [vp]
+    lib.harm_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]
+    lib.harm_step.argtypes = [vp, ctypes.c_int]
+    lib.harm_sync.argtypes = [vp, ctypes.POINTER(_Status)]
+    lib.harm_get_fluxes.argtypes = [vp, dp, dp]
+    lib.harm_destroy.argtypes = [vp]
+    lib.harm_destroy.restype = None
+    lib.harm_error_string.argtypes = [ctypes.c_int]
+    lib.harm_error_string.restype = ctypes.c_char_p
+    lib.harm_torus_default_params.argtypes = [ctypes.POINTER(_TorusParams)]
+    lib.harm_torus_default_params.restype = None
+    lib.harm_torus_geometry.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp, dp, dp]
+    lib.harm_torus_init.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
+    lib.harm_profile_step.argtypes = [vp, dp, ip, ctypes.c_int]
+    lib.harm_kernel_name.argtypes = [ctypes.c_int]
+    lib.harm_kernel_name.restype = ctypes.c_char_p
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise HarmError(rc, what)
+
+
+# ----------------------------------------------------------------- set-up
+def torus_params(n1=128, n2=128, **kw):
+    """The benchmark torus parameters (include/harm_setup.h) with overrides."""
+    lib = load_library()
+    p = _TorusParams()
+    lib.harm_torus_default_params(ctypes.byref(p))
+    p.n1, p.n2 = n1, n2
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def torus_geometry(params):
+    """set_grid() for the torus grid: dict of gcov, gcon, gdet, conn, floors
+    and the grid scalars (startx1, startx2, dx1, dx2, Rin, Rhor)."""
+    lib = load_library()
+    n1m, n2m = params.n1 + 2 * NG, params.n2 + 2 * NG
+    g = dict(gcov=np.zeros((n1m, n2m, 4, 4, 4)), gcon=np.zeros((n1m, n2m, 4, 4, 4)), gdet=np.zeros((n1m, n2m, 4)),
+             conn=np.zeros((n1m, n2m, 4, 4, 4)), floors=np.zeros((n1m, n2m, 2)))
+    grid = np.zeros(6)
+    _check(lib.harm_torus_geometry(ctypes.byref(params), _dp(g["gcov"]), _dp(g["gcon"]), _dp(g["gdet"]),
+                                   _dp(g["conn"]), _dp(g["floors"]), _dp(grid)), "harm_torus_geometry")
+    g.update(startx1=grid[0], startx2=grid[1], dx1=grid[2], dx2=grid[3], Rin=grid[4], Rhor=grid[5])
+    return g
+
+
+def torus_init(params, geom):
+    """init() for the torus: active-zone primitives (ghosts still to bound)."""
+    lib = load_library()
+    n1m, n2m = params.n1 + 2 * NG, params.n2 + 2 * NG
+    p = np.zeros((n1m, n2m, NPR))
+    _check(lib.harm_torus_init(ctypes.byref(params), _dp(geom["gcov"]), _dp(geom["gcon"]), _dp(geom["gdet"]),
+                               _dp(p)), "harm_torus_init")
+    return p
+
+
+# ----------------------------------------------------------------- device
+class HarmGPU:
+    """Device-resident state of the reference's step and its step_ch()."""
+
+    def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
+                 defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
+                 stream=None):
+        self.lib = load_library()
+        self.n1, self.n2 = n1, n2
+        self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
+        cfg = _Config(n1, n2, lim, fluxmethod, 0, 0, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+                      bsqorholimit, bsqoulimit, tf)
+        h = ctypes.c_void_p()
+        _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.harm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload_geometry(self, gcov, gcon, gdet, conn, floors):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (gcov, gcon, gdet, conn, floors)]
+        _check(self.lib.harm_upload_geometry(self._h, *[_dp(x) for x in arrs]), "harm_upload_geometry")
+
+    def set_prims(self, prims, pflag=None, reset_gammacheck=True):
+        p = np.ascontiguousarray(prims, dtype=np.float64)
+        assert p.shape == (self.n1m, self.n2m, NPR)
+        f = None if pflag is None else np.ascontiguousarray(pflag, dtype=np.int32)
+        _check(self.lib.harm_set_prims(self._h, _dp(p), None if f is None else _ip(f), int(bool(reset_gammacheck))),
+               "harm_set_prims")
+
+    def get_prims(self):
+        p = np.zeros((self.n1m, self.n2m, NPR))
+        f = np.zeros((self.n1m, self.n2m, 5), dtype=np.int32)
+        _check(self.lib.harm_get_prims(self._h, _dp(p), _ip(f)), "harm_get_prims")
+        return p, f
+
+    def bound_prims(self):
+        _check(self.lib.harm_bound_prims(self._h), "harm_bound_prims")
+
+    def set_time(self, t, dt, realnstep=0):
+        _check(self.lib.harm_set_time(self._h, t, dt, realnstep), "harm_set_time")
+
+    def step_ch(self, nsteps=1):
+        """Enqueue nsteps reference steps (asynchronous)."""
+        _check(self.lib.harm_step(self._h, int(nsteps)), "harm_step")
+
+    def sync(self, raise_on_fail=True):
+        st = _Status()
+        rc = self.lib.harm_sync(self._h, ctypes.byref(st))
+        d = dict(fail_code=st.fail_code, fail_i=st.fail_i, fail_j=st.fail_j, fixups=st.fixups,
+                 realnstep=st.realnstep, t=st.t, dt=st.dt, newton_iters=st.newton_iters)
+        if rc == 6 and raise_on_fail:
+            raise HarmError(rc, f"step failed with {FAIL_NAMES.get(st.fail_code, st.fail_code)} at zone "
+                                f"({st.fail_i},{st.fail_j})")
+        if rc not in (0, 6):
+            raise HarmError(rc, "harm_sync")
+        return d
+
+    def profile_step(self):
+        """One step with a CUDA event after every kernel: {name: (ms, launches)}."""
+        nk = 12
+        ms = np.zeros(nk)
+        n = np.zeros(nk, dtype=np.int32)
+        _check(self.lib.harm_profile_step(self._h, _dp(ms), _ip(n), nk), "harm_profile_step")
+        return {self.lib.harm_kernel_name(k).decode(): (float(ms[k]), int(n[k])) for k in range(nk)}
+
+    def get_fluxes(self):
+        f1 = np.zeros((self.n1m, self.n2m, NPR))
+        f2 = np.zeros((self.n1m, self.n2m, NPR))
+        _check(self.lib.harm_get_fluxes(self._h, _dp(f1), _dp(f2)), "harm_get_fluxes")
+        return f1, f2
+
+
+def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, stream=None, **torus_kw):
+    """Builds the benchmark torus on the host and returns (HarmGPU, geometry,
+    initial prims) with the state uploaded, bounded and t=0, dt=1e-5 set as
+    init_defglobal() leaves them (initbase.c:158)."""
+    par = torus_params(n1, n2, **torus_kw)
+    geom = torus_geometry(par)
+    p0 = torus_init(par, geom)
+    h = HarmGPU(n1, n2, geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, cour=cour, gam=par.gam,
+                gammamax=par.gammamax, stream=stream)
+    h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
+    h.set_prims(p0)
+    h.bound_prims()
+    h.set_time(0.0, 1.0e-5, 0)
+    return h, geom, p0

@@ -1,0 +1,497 @@
+// Host engine and C ABI (include/harm_b200.h) of the B200 HARM step.
+//
+// The engine owns the device arrays (structure-of-arrays planes, see
+// harm_kernels.cuh), converts the reference-layout host arrays on upload and
+// download, and enqueues one step of step_ch() (step_ch.c:35-188 with the
+// midpoint RK2 of setup_rktimestep, step_ch.c:412-429) as a fixed sequence
+// of kernels on its stream.  The sequence is captured once into a CUDA graph
+// and replayed; dt and t live in device memory, so steps chain without host
+// round trips.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+#include "../../include/harm_b200.h"
+#include "harm_kernels.cuh"
+
+namespace harm {
+__global__ void k_bsqflags(StepArgs a, const double* pv);
+void launch_flux(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+__global__ void k_emf(StepArgs a);
+void launch_update(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb, double* pf,
+                   double c2);
+__global__ void k_bound(StepArgs a, double* pv, int with_pflag);
+__global__ void k_poledeath(StepArgs a, double* pv);
+__global__ void k_gammacheck(StepArgs a, const double* pv);
+__global__ void k_checksol(StepArgs a, const double* pv, int round);
+__global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
+__global__ void k_fixup_compute(StepArgs a, const double* pv);
+__global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd);
+__global__ void k_dt_finalize(StepArgs a);
+}  // namespace harm
+
+using namespace harm;
+
+static const int CHK_ROUNDS = 4;
+
+struct harm_ctx {
+  harm_config cfg;
+  cudaStream_t stream;
+  Grid gr;
+  int n1m, n2m;
+  // device buffers
+  double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin;
+  int* d_pflag;
+  unsigned char *d_bsqf, *d_chk;
+  DevScalars* d_sc;
+  int nblocks_flux;
+  bool geo_ok;
+  cudaGraph_t graph;
+  cudaGraphExec_t gexec;
+  bool have_graph;
+  StepArgs args() const
+  {
+    StepArgs a;
+    a.gr = gr;
+    a.pp.lim = cfg.lim;
+    a.pp.fluxmethod = cfg.fluxmethod;
+    a.pp.cour = cfg.cour;
+    a.pp.gam = cfg.gam;
+    a.pp.dx1 = cfg.dx1;
+    a.pp.dx2 = cfg.dx2;
+    a.pp.safe = cfg.safe;
+    a.pp.defcon = cfg.defcon;
+    a.pp.gammamax = cfg.gammamax;
+    a.pp.gammafail = cfg.gammafail;
+    a.pp.bsqorholimit = cfg.bsqorholimit;
+    a.pp.bsqoulimit = cfg.bsqoulimit;
+    a.pp.tf = cfg.tf;
+    a.geo = d_geo;
+    a.F1 = d_F1;
+    a.F2 = d_F2;
+    a.emf = d_emf;
+    a.pflag = d_pflag;
+    a.bsqf = d_bsqf;
+    a.gammacheck = d_gammacheck;
+    a.chk = d_chk;
+    a.fixbuf = d_fixbuf;
+    a.blockmin = d_blockmin;
+    a.nblocks_flux = nblocks_flux;
+    a.sc = d_sc;
+    return a;
+  }
+};
+
+#define CK(call)                                     \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) {                         \
+      fprintf(stderr, "harm_b200: %s: %s\n", #call, cudaGetErrorString(e_)); \
+      return HARM_ECUDA;                             \
+    }                                                \
+  } while (0)
+
+static dim3 grid2(int ni, int nj, dim3 b) { return dim3((ni + b.x - 1) / b.x, (nj + b.y - 1) / b.y); }
+
+// kernel classes of one step, in launch order (for per-kernel timing)
+enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_CHECKSOL, KC_CHECKSERIAL, KC_FIXC,
+       KC_FIXA, KC_DT, KC_COUNT };
+static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", "k_update", "k_bound", "k_poledeath",
+                                               "k_gammacheck", "k_checksol", "k_checksol_serial", "k_fixup_compute",
+                                               "k_fixup_apply", "k_dt_finalize"};
+
+struct Timer {
+  // records an event after every launch when active
+  cudaEvent_t ev[64];
+  int cls[64];
+  int n = 0;
+  bool on = false;
+  void mark(cudaStream_t s, int k)
+  {
+    if (!on || n >= 63) return;
+    cudaEventRecord(ev[n + 1], s);
+    cls[n + 1] = k;
+    n++;
+  }
+};
+
+static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
+{
+  Timer dummy;
+  Timer& T = tm ? *tm : dummy;
+  const StepArgs a = c->args();
+  const int n1 = c->cfg.n1, n2 = c->cfg.n2;
+  const dim3 b(32, 4);
+  cudaStream_t s = c->stream;
+  k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
+  T.mark(s, KC_BSQ);
+  for (int sub = 0; sub < 2; sub++) {
+    const double* pi = c->d_p;
+    const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
+    double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
+    const double c2 = (sub == 0) ? 0.5 : 1.0;
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
+    T.mark(s, KC_FLUX);
+    k_emf<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a);
+    T.mark(s, KC_EMF);
+    launch_update(grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
+    T.mark(s, KC_UPDATE);
+    k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
+    T.mark(s, KC_BOUND);
+    k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
+    T.mark(s, KC_POLE);
+    k_gammacheck<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pf);
+    T.mark(s, KC_GCHECK);
+    for (int r = 0; r < CHK_ROUNDS; r++) {
+      k_checksol<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, r);
+      T.mark(s, KC_CHECKSOL);
+    }
+    k_checksol_serial<<<1, 32, 0, s>>>(a, pf, CHK_ROUNDS);
+    T.mark(s, KC_CHECKSERIAL);
+    k_fixup_compute<<<grid2(n1, n2, b), b, 0, s>>>(a, pf);
+    T.mark(s, KC_FIXC);
+    k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, c->cfg.eom == HARM_EOM_GRMHD);
+    T.mark(s, KC_FIXA);
+    k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 0);
+    T.mark(s, KC_BOUND);
+    k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
+    T.mark(s, KC_POLE);
+  }
+  k_dt_finalize<<<1, 1024, 0, s>>>(a);
+  T.mark(s, KC_DT);
+  return cudaGetLastError() == cudaSuccess ? HARM_OK : HARM_ECUDA;
+}
+
+extern "C" {
+
+const char* harm_error_string(int code)
+{
+  switch (code) {
+    case HARM_OK: return "ok";
+    case HARM_EINVAL: return "invalid argument";
+    case HARM_ENODEVICE: return "no usable CUDA device (sm_100 required)";
+    case HARM_ECUDA: return "CUDA runtime error";
+    case HARM_ENOMEM: return "device allocation failed";
+    case HARM_EGEOMETRY: return "geometry tables missing or not symmetric";
+    case HARM_EFAIL: return "fatal check of the reference step fired";
+    default: return "unknown error";
+  }
+}
+
+int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
+{
+  if (!cfg || !out) return HARM_EINVAL;
+  *out = nullptr;
+  if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->reserved != 0) return HARM_EINVAL;
+  if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
+  if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
+  if (cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
+  int dev = 0, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HARM_ENODEVICE;
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major != 10) return HARM_ENODEVICE;
+  harm_ctx* c = new harm_ctx();
+  memset(c, 0, sizeof(*c));
+  c->cfg = *cfg;
+  c->stream = (cudaStream_t)stream;
+  c->n1m = cfg->n1 + 2 * NG;
+  c->n2m = cfg->n2 + 2 * NG;
+  c->gr.n1 = cfg->n1;
+  c->gr.n2 = cfg->n2;
+  c->gr.pitch = ((c->n1m + 15) / 16) * 16;
+  c->gr.rows = c->n2m;
+  c->gr.plane = (long long)c->gr.pitch * c->gr.rows;
+  const size_t pd = (size_t)c->gr.plane * sizeof(double);
+  const dim3 b(32, 4);
+  dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, b);
+  c->nblocks_flux = gf.x * gf.y;
+  bool ok = true;
+  ok &= cudaMalloc(&c->d_p, NPR * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_pk0, NPR * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_geo, GEO_NPLANES * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_F1, NPR * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_F2, NPR * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_emf, pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_gammacheck, pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_fixbuf, 5 * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_blockmin, 2 * (size_t)c->nblocks_flux * sizeof(double)) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_pflag, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_bsqf, (size_t)c->gr.plane) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_chk, 2 * (size_t)c->gr.plane) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_sc, sizeof(DevScalars)) == cudaSuccess;
+  if (!ok) {
+    harm_destroy(c);
+    return HARM_ENOMEM;
+  }
+  cudaMemsetAsync(c->d_p, 0, NPR * pd, c->stream);
+  cudaMemsetAsync(c->d_pk0, 0, NPR * pd, c->stream);
+  cudaMemsetAsync(c->d_geo, 0, GEO_NPLANES * pd, c->stream);
+  cudaMemsetAsync(c->d_F1, 0, NPR * pd, c->stream);
+  cudaMemsetAsync(c->d_F2, 0, NPR * pd, c->stream);
+  cudaMemsetAsync(c->d_emf, 0, pd, c->stream);
+  cudaMemsetAsync(c->d_gammacheck, 0, pd, c->stream);
+  cudaMemsetAsync(c->d_fixbuf, 0, 5 * pd, c->stream);
+  cudaMemsetAsync(c->d_pflag, 0, (size_t)c->gr.plane * sizeof(int), c->stream);
+  cudaMemsetAsync(c->d_bsqf, 0, (size_t)c->gr.plane, c->stream);
+  cudaMemsetAsync(c->d_chk, 0, 2 * (size_t)c->gr.plane, c->stream);
+  cudaMemsetAsync(c->d_sc, 0, sizeof(DevScalars), c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    harm_destroy(c);
+    return HARM_ECUDA;
+  }
+  *out = c;
+  return HARM_OK;
+}
+
+void harm_destroy(harm_ctx* c)
+{
+  if (!c) return;
+  if (c->have_graph) {
+    cudaGraphExecDestroy(c->gexec);
+    cudaGraphDestroy(c->graph);
+  }
+  cudaFree(c->d_p);
+  cudaFree(c->d_pk0);
+  cudaFree(c->d_geo);
+  cudaFree(c->d_F1);
+  cudaFree(c->d_F2);
+  cudaFree(c->d_emf);
+  cudaFree(c->d_gammacheck);
+  cudaFree(c->d_fixbuf);
+  cudaFree(c->d_blockmin);
+  cudaFree(c->d_pflag);
+  cudaFree(c->d_bsqf);
+  cudaFree(c->d_chk);
+  cudaFree(c->d_sc);
+  delete c;
+}
+
+int harm_upload_geometry(harm_ctx* c, const double* gcov, const double* gcon, const double* gdet, const double* conn,
+                         const double* floors)
+{
+  if (!c || !gcov || !gcon || !gdet || !conn || !floors) return HARM_EINVAL;
+  const int n1m = c->n1m, n2m = c->n2m;
+  const long long pl = c->gr.plane;
+  std::vector<double> h((size_t)GEO_NPLANES * pl, 0.0);
+  for (int ii = 0; ii < n1m; ii++)
+    for (int jj = 0; jj < n2m; jj++) {
+      const long long zr = (long long)ii * n2m + jj;                 // reference zone
+      const long long zd = c->gr.at(ii - NG, jj - NG);               // device zone
+      for (int loc = 0; loc < 4; loc++) {
+        const double* gv = gcov + (zr * 4 + loc) * 16;
+        const double* gn = gcon + (zr * 4 + loc) * 16;
+        for (int a = 0; a < 4; a++)
+          for (int b = a; b < 4; b++) {
+            // the step kernels use the packed symmetric form; the reference
+            // reads both triangles, so they must agree bit for bit
+            if (gv[a * 4 + b] != gv[b * 4 + a] || gn[a * 4 + b] != gn[b * 4 + a]) return HARM_EGEOMETRY;
+            h[((size_t)loc * GEO_PER_LOC + sym(a, b)) * pl + zd] = gv[a * 4 + b];
+            h[((size_t)loc * GEO_PER_LOC + 10 + sym(a, b)) * pl + zd] = gn[a * 4 + b];
+          }
+        h[((size_t)loc * GEO_PER_LOC + 20) * pl + zd] = gdet[zr * 4 + loc];
+      }
+      const double* cn = conn + zr * 64;
+      for (int k = 0; k < 4; k++)
+        for (int l = 0; l < 4; l++)
+          for (int j = l; j < 4; j++) {
+            if (cn[(k * 4 + l) * 4 + j] != cn[(k * 4 + j) * 4 + l]) return HARM_EGEOMETRY;
+            h[(size_t)conn_plane(k, l, j) * pl + zd] = cn[(k * 4 + l) * 4 + j];
+          }
+      h[(size_t)GEO_FLOOR * pl + zd] = floors[zr * 2 + 0];
+      h[(size_t)(GEO_FLOOR + 1) * pl + zd] = floors[zr * 2 + 1];
+    }
+  CK(cudaMemcpyAsync(c->d_geo, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->geo_ok = true;
+  return HARM_OK;
+}
+
+int harm_set_prims(harm_ctx* c, const double* prims, const int* pflag, int reset_gammacheck)
+{
+  if (!c || !prims) return HARM_EINVAL;
+  const int n1m = c->n1m, n2m = c->n2m;
+  const long long pl = c->gr.plane;
+  std::vector<double> h((size_t)NPR * pl, 0.0);
+  std::vector<int> hf((size_t)pl, 0);
+  for (int ii = 0; ii < n1m; ii++)
+    for (int jj = 0; jj < n2m; jj++) {
+      const long long zr = (long long)ii * n2m + jj, zd = c->gr.at(ii - NG, jj - NG);
+      for (int k = 0; k < NPR; k++) h[(size_t)k * pl + zd] = prims[zr * NPR + k];
+      if (pflag) hf[zd] = pflag[zr * 5 + 0];
+    }
+  CK(cudaMemcpyAsync(c->d_p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_pflag, hf.data(), hf.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (reset_gammacheck) CK(cudaMemsetAsync(c->d_gammacheck, 0, (size_t)pl * sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return HARM_OK;
+}
+
+int harm_get_prims(harm_ctx* c, double* prims, int* pflag)
+{
+  if (!c) return HARM_EINVAL;
+  const int n1m = c->n1m, n2m = c->n2m;
+  const long long pl = c->gr.plane;
+  std::vector<double> h((size_t)NPR * pl);
+  std::vector<int> hf((size_t)pl);
+  std::vector<unsigned char> hb((size_t)pl);
+  CK(cudaMemcpyAsync(h.data(), c->d_p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hf.data(), c->d_pflag, hf.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hb.data(), c->d_bsqf, hb.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int ii = 0; ii < n1m; ii++)
+    for (int jj = 0; jj < n2m; jj++) {
+      const long long zr = (long long)ii * n2m + jj, zd = c->gr.at(ii - NG, jj - NG);
+      if (prims)
+        for (int k = 0; k < NPR; k++) prims[zr * NPR + k] = h[(size_t)k * pl + zd];
+      if (pflag) {
+        pflag[zr * 5 + 0] = hf[zd];
+        pflag[zr * 5 + 1] = 0;
+        pflag[zr * 5 + 2] = hb[zd] & 3;
+        pflag[zr * 5 + 3] = (hb[zd] >> 2) & 3;
+        pflag[zr * 5 + 4] = 0;
+      }
+    }
+  return HARM_OK;
+}
+
+int harm_bound_prims(harm_ctx* c)
+{
+  if (!c) return HARM_EINVAL;
+  if (!c->geo_ok) return HARM_EGEOMETRY;
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  k_bound<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, c->stream>>>(a, c->d_p, 1);
+  k_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, c->stream>>>(a, c->d_p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return HARM_OK;
+}
+
+int harm_set_time(harm_ctx* c, double t, double dt, long long realnstep)
+{
+  if (!c) return HARM_EINVAL;
+  DevScalars h;
+  memset(&h, 0, sizeof(h));
+  h.t = t;
+  h.dt = dt;
+  h.realnstep = realnstep;
+  CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return HARM_OK;
+}
+
+int harm_step(harm_ctx* c, int nsteps)
+{
+  if (!c || nsteps < 0) return HARM_EINVAL;
+  if (!c->geo_ok) return HARM_EGEOMETRY;
+  if (!c->have_graph) {
+    cudaStream_t cap = c->stream;
+    bool own = false;
+    if (cap == 0) {
+      // the legacy default stream cannot be captured: capture on a private one
+      CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      own = true;
+    }
+    harm_ctx tmp = *c;
+    tmp.stream = cap;
+    CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(&tmp);
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamEndCapture(cap, &g);
+    if (own) cudaStreamDestroy(cap);
+    if (rc != HARM_OK || e != cudaSuccess) return HARM_ECUDA;
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    c->graph = g;
+    c->have_graph = true;
+  }
+  for (int n = 0; n < nsteps; n++) CK(cudaGraphLaunch(c->gexec, c->stream));
+  return HARM_OK;
+}
+
+int harm_sync(harm_ctx* c, harm_status* st)
+{
+  if (!c) return HARM_EINVAL;
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    st->fail_code = h.status;
+    st->fail_i = h.status ? (h.status_zone % 100000) - NG : 0;
+    st->fail_j = h.status ? (h.status_zone / 100000) - NG : 0;
+    st->fixups = h.fixups;
+    st->realnstep = h.realnstep;
+    st->t = h.t;
+    st->dt = h.dt;
+    st->newton_iters = h.newton_iters;
+  }
+  return h.status ? HARM_EFAIL : HARM_OK;
+}
+
+int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)
+{
+  if (!c || !ms || !launches || nclasses < KC_COUNT) return HARM_EINVAL;
+  if (!c->geo_ok) return HARM_EGEOMETRY;
+  Timer T;
+  for (int k = 0; k < 64; k++) CK(cudaEventCreate(&T.ev[k]));
+  T.on = true;
+  CK(cudaEventRecord(T.ev[0], c->stream));
+  int rc = enqueue_step(c, &T);
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < nclasses; k++) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  for (int k = 1; k <= T.n; k++) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, T.ev[k - 1], T.ev[k]);
+    ms[T.cls[k]] += t;
+    launches[T.cls[k]] += 1;
+  }
+  for (int k = 0; k < 64; k++) cudaEventDestroy(T.ev[k]);
+  return rc;
+}
+
+const char* harm_kernel_name(int k) { return (k >= 0 && k < KC_COUNT) ? KC_NAMES[k] : ""; }
+
+int harm_get_fluxes(harm_ctx* c, double* F1, double* F2)
+{
+  if (!c || !F1 || !F2) return HARM_EINVAL;
+  const int n1 = c->cfg.n1, n2 = c->cfg.n2, n1m = c->n1m, n2m = c->n2m;
+  const long long pl = c->gr.plane;
+  std::vector<double> h1((size_t)NPR * pl), h2((size_t)NPR * pl), he((size_t)pl);
+  CK(cudaMemcpyAsync(h1.data(), c->d_F1, h1.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(h2.data(), c->d_F2, h2.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(he.data(), c->d_emf, he.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  auto D = [&](int i, int j) { return c->gr.at(i, j); };
+  auto R = [&](int i, int j) { return ((long long)(i + NG) * n2m + (j + NG)) * NPR; };
+  for (int ii = 0; ii < n1m; ii++)
+    for (int jj = 0; jj < n2m; jj++)
+      for (int k = 0; k < NPR; k++) {
+        F1[((long long)ii * n2m + jj) * NPR + k] = h1[(size_t)k * pl + D(ii - NG, jj - NG)];
+        F2[((long long)ii * n2m + jj) * NPR + k] = h2[(size_t)k * pl + D(ii - NG, jj - NG)];
+      }
+  // fix_flux's mirrored B2 on the x2 ghost rows (fixup.c:1369-1381)
+  for (int i = -1; i < n1; i++) {
+    F1[R(i, -1) + B2] = -F1[R(i, 0) + B2];
+    F1[R(i, n2) + B2] = -F1[R(i, n2 - 1) + B2];
+  }
+  // flux-CT rewrite, step_ch.c:1403-1413
+  for (int i = 0; i <= n1; i++)
+    for (int j = 0; j <= n2 - 1; j++) {
+      F1[R(i, j) + B1] = 0.;
+      F1[R(i, j) + B2] = 0.5 * (he[D(i, j)] + he[D(i, j + 1)]);
+    }
+  for (int i = 0; i <= n1 - 1; i++)
+    for (int j = 0; j <= n2; j++) {
+      F2[R(i, j) + B1] = -0.5 * (he[D(i, j)] + he[D(i + 1, j)]);
+      F2[R(i, j) + B2] = 0.;
+    }
+  return HARM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// HARM step kernels for sm_100a.
+//
+// Data layout in HBM (structure of arrays, x1 index i fastest):
+//   a field plane holds one double per zone over the full grid including
+//   NG = 3 ghost zones per side; zone (i, j), i in [-3, n1+3), j in [-3, n2+3),
+//   sits at (j+3)*pitch + (i+3), with pitch = n1+6 rounded up to 16 doubles
+//   (128 B rows).  Primitive state: 8 consecutive planes (rho, u, u~1..3,
+//   B1..3).  Geometry: per location (FACE1, FACE2, CORN, CENT) 10 gcov + 10
+//   gcon + 1 gdet planes; 40 connection planes Gamma^k_{(lj)} at CENT; 2 floor
+//   planes.  Fluxes: 8 planes per direction.
+#pragma once
+#include "harm_device.cuh"
+
+namespace harm {
+
+constexpr int NG = 3;
+
+struct Grid {
+  int n1, n2;    // interior zones
+  int pitch;     // doubles per row (i direction, with ghosts)
+  int rows;      // n2 + 2*NG
+  long long plane;
+  __host__ __device__ __forceinline__ long long at(int i, int j) const { return (long long)(j + NG) * pitch + (i + NG); }
+};
+
+// geometry plane offsets inside the geometry block
+constexpr int GEO_PER_LOC = 21;                 // 10 gcov, 10 gcon, gdet
+constexpr int GEO_CONN = 4 * GEO_PER_LOC;       // 40 connection planes follow
+constexpr int GEO_FLOOR = GEO_CONN + 40;        // 2 floor planes
+constexpr int GEO_NPLANES = GEO_FLOOR + 2;
+
+__host__ __device__ constexpr int conn_plane(int k, int l, int j) { return GEO_CONN + k * 10 + sym(l, j); }
+
+struct Params {
+  int lim;          // 3 MC, 4 PARA
+  int fluxmethod;   // 0 LAXF, 1 HLL
+  double cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit, tf;
+};
+
+// device-resident scalars of the run (one struct in device memory)
+struct DevScalars {
+  double t, dt, ndt;
+  long long realnstep;
+  int status;            // first fatal fail code (0 = ok)
+  int status_zone;       // i + (n1+6)*j of the first failure (+ offsets)
+  unsigned long long newton_iters;   // Newton iterations since the last reset
+  int chk_changed[8];    // per-round change flags of the check-solution sweep
+  int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
+  int fixups;            // zones repaired by fixup_utoprim in the last step
+};
+
+struct StepArgs {
+  Grid gr;
+  Params pp;
+  const double* geo;     // GEO_NPLANES planes
+  double* F1;            // 8 planes
+  double* F2;            // 8 planes
+  double* emf;           // 1 plane
+  int* pflag;            // 1 plane (FLAGUTOPRIMFAIL)
+  unsigned char* bsqf;   // 1 plane: (b^2/rho flag) | (b^2/u flag) << 2
+  double* gammacheck;    // 1 plane, persistent
+  unsigned char* chk;    // 2 planes: check-solution decisions (double buffer)
+  double* fixbuf;        // 5 planes: repaired rho..u3
+  double* blockmin;      // per-block dt minima: [2][nblocks]
+  int nblocks_flux;
+  DevScalars* sc;
+};
+
+__device__ __forceinline__ void report_fail(DevScalars* sc, int code, int i, int j)
+{
+  if (atomicCAS(&sc->status, 0, code) == 0) sc->status_zone = (i + NG) + 100000 * (j + NG);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_geo(const StepArgs& a, int loc, long long z, Geo<T>& g)
+{
+  const double* base = a.geo + (long long)loc * GEO_PER_LOC * a.gr.plane + z;
+#pragma unroll
+  for (int c = 0; c < 10; c++) g.gcov[c] = (T)__ldg(base + c * a.gr.plane);
+#pragma unroll
+  for (int c = 0; c < 10; c++) g.gcon[c] = (T)__ldg(base + (10 + c) * a.gr.plane);
+  g.g = (T)__ldg(base + 20 * a.gr.plane);
+}
+
+__device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long z)
+{
+  return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
+}
+
+}  // namespace harm

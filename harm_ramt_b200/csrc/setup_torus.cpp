@@ -1,0 +1,661 @@
+// Host-side plugin surface for standalone runs: the modified Kerr-Schild
+// grid and the Fishbone-Moncrief torus that the reference builds in
+// coord.c / metric.c / set_grid.c / init.fishmon.c / initbase.c.
+//
+// This is set-up code (run once, on the host), not the step: it produces the
+// geometry tables and the initial primitive state in the reference layout
+// that harm_upload_geometry() / harm_set_prims() take.  The arithmetic
+// follows the reference's evaluation order so that the geometry agrees with
+// the reference bit for bit.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/harm_b200.h"
+#include "../../include/harm_setup.h"
+
+namespace {
+
+constexpr int NG = 3;
+constexpr int FACE1 = 0, FACE2 = 1, CORN = 2, CENT = 3;
+enum { RHO = 0, UU, U1, U2, U3, B1, B2, B3 };
+
+struct Coords {
+  double a, R0, Rin, Rout, hslope, startx1, startx2, dx1, dx2;
+};
+
+// coord(), coord.c:920-938
+void coord_of(const Coords& c, int i, int j, int loc, double* X)
+{
+  if (loc == FACE1) {
+    X[1] = c.startx1 + (i + 0) * c.dx1;
+    X[2] = c.startx2 + ((j + 0) + 0.5) * c.dx2;
+  } else if (loc == FACE2) {
+    X[1] = c.startx1 + ((i + 0) + 0.5) * c.dx1;
+    X[2] = c.startx2 + (j + 0) * c.dx2;
+  } else if (loc == CENT) {
+    X[1] = c.startx1 + ((i + 0) + 0.5) * c.dx1;
+    X[2] = c.startx2 + ((j + 0) + 0.5) * c.dx2;
+  } else {
+    X[1] = c.startx1 + (i + 0) * c.dx1;
+    X[2] = c.startx2 + (j + 0) * c.dx2;
+  }
+  X[0] = X[3] = 0.0;
+}
+
+// bl_coord for defcoord 0 with COORDSINGFIX, coord.c:334-453
+void bl_of(const Coords& c, const double* X, double* r, double* th)
+{
+  *r = c.R0 + exp(X[1]);
+  *th = M_PI * X[2] + ((1. - c.hslope) / 2.) * sin(2. * M_PI * X[2]);
+  if (fabs(*th) < 1E-20) {
+    if (*th >= 0) *th = 1E-20;
+    if (*th < 0) *th = -1E-20;
+  }
+}
+
+// dxdxp_analytic defcoord 0 (diagonal), coord.c:480-491
+void dxdxp_of(const Coords& c, const double* X, double r, double d[4])
+{
+  d[0] = 1.0;
+  d[1] = r - c.R0;
+  d[2] = M_PI + (1. - c.hslope) * M_PI * cos(2. * M_PI * X[2]);
+  d[3] = 1.0;
+}
+
+// set_gcov_ksmetric (metric.c:540-597) then gcov2gcovprim (metric.c:1057-1083)
+// with the diagonal Jacobian: g'_{jk} = (g_{jk} d_j) d_k
+void gcov_prim(const Coords& c, const double* X, double g[4][4])
+{
+  double r, th;
+  bl_of(c, X, &r, &th);
+  const double a = c.a;
+  const double cth = cos(th), sth = sin(th), s2 = sth * sth;
+  const double rho2 = r * r + a * a * cth * cth;
+  double ks[4][4];
+  ks[0][0] = (-1. + 2. * r / rho2);
+  ks[0][1] = (2. * r / rho2);
+  ks[0][2] = (0);
+  ks[0][3] = (-2. * a * r * s2 / rho2);
+  ks[1][0] = ks[0][1];
+  ks[1][1] = (1. + 2. * r / rho2);
+  ks[1][2] = (0);
+  ks[1][3] = (-a * s2 * (1. + 2. * r / rho2));
+  ks[2][0] = (0);
+  ks[2][1] = (0);
+  ks[2][2] = (rho2);
+  ks[2][3] = (0);
+  ks[3][0] = ks[0][3];
+  ks[3][1] = ks[1][3];
+  ks[3][2] = (0);
+  ks[3][3] = (s2 * (rho2 + a * a * s2 * (1. + 2. * r / rho2)));
+  double d[4];
+  dxdxp_of(c, X, r, d);
+  double dm[4][4] = {{0}};
+  for (int k = 0; k < 4; k++) dm[k][k] = d[k];
+  for (int j = 0; j < 4; j++)
+    for (int k = 0; k < 4; k++) {
+      double t = 0.;
+      for (int l = 0; l < 4; l++)
+        for (int m = 0; m < 4; m++) t += ks[l][m] * dm[l][j] * dm[m][k];
+      g[j][k] = t;
+    }
+}
+
+// set_gcon_ksmetric (metric.c:666-722) then gcon2gconprim (metric.c:1085-1106);
+// the inverse Jacobian of a diagonal matrix is its reciprocal diagonal
+// (which the reference's Gauss-Jordan produces exactly: pivot 1/d_kk).
+void gcon_prim(const Coords& c, const double* X, double g[4][4])
+{
+  double r, th;
+  bl_of(c, X, &r, &th);
+  const double a = c.a;
+  const double cth = cos(th), sth = sin(th), s2 = sth * sth;
+  const double rho2 = r * r + a * a * cth * cth;
+  double ks[4][4];
+  ks[0][0] = (-(1. + 2. * r / rho2));
+  ks[0][1] = (2. * r / rho2);
+  ks[0][2] = (0);
+  ks[0][3] = (0);
+  ks[1][0] = ks[0][1];
+  ks[1][1] = ((r * (r - 2.) + a * a) / rho2);
+  ks[1][2] = (0);
+  ks[1][3] = (a / rho2);
+  ks[2][0] = ks[0][2];
+  ks[2][1] = ks[1][2];
+  ks[2][2] = (1. / rho2);
+  ks[2][3] = (0);
+  ks[3][0] = ks[0][3];
+  ks[3][1] = ks[1][3];
+  ks[3][2] = ks[2][3];
+  ks[3][3] = (1. / (rho2 * s2));
+  double d[4];
+  dxdxp_of(c, X, r, d);
+  double id[4][4] = {{0}};
+  for (int k = 0; k < 4; k++) id[k][k] = 1.0 / d[k];
+  for (int j = 0; j < 4; j++)
+    for (int k = 0; k < 4; k++) {
+      double t = 0.;
+      for (int l = 0; l < 4; l++)
+        for (int m = 0; m < 4; m++) t += id[j][l] * id[k][m] * ks[l][m];
+      g[j][k] = t;
+    }
+}
+
+// gdet_func, metric.c:1109-1140: LU decomposition with implicit partial
+// pivoting (the Numerical Recipes ludcmp of ludcmp.c), det = d * prod(diag)
+double gdet_of(const double gin[4][4])
+{
+  double a[5][5], vv[5], d = 1.0;
+  for (int j = 0; j < 4; j++)
+    for (int k = 0; k < 4; k++) a[j + 1][k + 1] = gin[j][k];
+  const int n = 4;
+  int imax = 0;
+  for (int i = 1; i <= n; i++) {
+    double big = 0.0, temp;
+    for (int j = 1; j <= n; j++)
+      if ((temp = fabs(a[i][j])) > big) big = temp;
+    if (big == 0.0) return NAN;
+    vv[i] = 1.0 / big;
+  }
+  for (int j = 1; j <= n; j++) {
+    for (int i = 1; i < j; i++) {
+      double sum = a[i][j];
+      for (int k = 1; k < i; k++) sum -= a[i][k] * a[k][j];
+      a[i][j] = sum;
+    }
+    double big = 0.0, dum;
+    for (int i = j; i <= n; i++) {
+      double sum = a[i][j];
+      for (int k = 1; k < j; k++) sum -= a[i][k] * a[k][j];
+      a[i][j] = sum;
+      if ((dum = vv[i] * fabs(sum)) >= big) {
+        big = dum;
+        imax = i;
+      }
+    }
+    if (j != imax) {
+      for (int k = 1; k <= n; k++) {
+        dum = a[imax][k];
+        a[imax][k] = a[j][k];
+        a[j][k] = dum;
+      }
+      d = -d;
+      vv[imax] = vv[j];
+    }
+    if (a[j][j] == 0.0) a[j][j] = 1.0e-30;
+    if (j != n) {
+      dum = 1.0 / (a[j][j]);
+      for (int i = j + 1; i <= n; i++) a[i][j] *= dum;
+    }
+  }
+  for (int j = 1; j <= n; j++) d *= a[j][j];
+  return (d >= 0) ? NAN : sqrt(-d);
+}
+
+// conn_func_numerical1 with GAMMIEDERIVATIVE and CONNDELTA 1e-5,
+// metric.c:1188-1262: centred differences of g'_{mu nu}, lowered Christoffel
+// symbols, then raised with g'^{mu nu} at CENT.  conn[k][l][j] = Gamma^k_{lj}.
+void conn_of(const Coords& c, const double* X, const double gcon[4][4], double conn[4][4][4])
+{
+  const double DELTA = 1E-5;
+  double dg[4][4][4], tmp[4][4][4];
+  for (int k = 0; k < 4; k++) {
+    double Xh[4], Xl[4], gh[4][4], gl[4][4];
+    for (int l = 0; l < 4; l++) Xh[l] = Xl[l] = X[l];
+    Xh[k] += DELTA;
+    Xl[k] -= DELTA;
+    gcov_prim(c, Xh, gh);
+    gcov_prim(c, Xl, gl);
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) dg[i][j][k] = (gh[i][j] - gl[i][j]) / (Xh[k] - Xl[k]);
+  }
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 4; k++) tmp[i][j][k] = 0.5 * (dg[j][i][k] + dg[k][i][j] - dg[k][j][i]);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 4; k++) {
+        double s = 0.;
+        for (int l = 0; l < 4; l++) s += gcon[i][l] * tmp[l][j][k];
+        conn[i][j][k] = s;
+      }
+}
+
+// ------------------------------------------------------------------ state
+struct G {
+  const double* gcov;  // 16
+  const double* gcon;  // 16
+  double g;
+};
+
+double gamma_of(const double* pr, const G& g)
+{
+  const double* c = g.gcov;
+  double qsq = c[5] * pr[U1] * pr[U1] + c[10] * pr[U2] * pr[U2] + c[15] * pr[U3] * pr[U3] +
+               2. * (c[6] * pr[U1] * pr[U2] + c[7] * pr[U1] * pr[U3] + c[11] * pr[U2] * pr[U3]);
+  return sqrt(1. + qsq);
+}
+
+void ucon_rel4(const double* pr, const G& g, double* ucon)
+{
+  double alpha = 1. / sqrt(-g.gcon[0]);
+  double b1 = g.gcon[1] * alpha * alpha, b2 = g.gcon[2] * alpha * alpha, b3 = g.gcon[3] * alpha * alpha;
+  double gamma = gamma_of(pr, g);
+  ucon[0] = gamma / alpha;
+  ucon[1] = pr[U1] - gamma * b1 / alpha;
+  ucon[2] = pr[U2] - gamma * b2 / alpha;
+  ucon[3] = pr[U3] - gamma * b3 / alpha;
+}
+
+void lower4(const double* v, const double* c, double* w)
+{
+  w[0] = c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3];
+  w[1] = c[1] * v[0] + c[5] * v[1] + c[6] * v[2] + c[7] * v[3];
+  w[2] = c[2] * v[0] + c[6] * v[1] + c[10] * v[2] + c[11] * v[3];
+  w[3] = c[3] * v[0] + c[7] * v[1] + c[11] * v[2] + c[15] * v[3];
+}
+
+double bsq_of(const double* pr, const G& g)
+{
+  double ucon[4], ucov[4], bcon[4], bcov[4];
+  ucon_rel4(pr, g, ucon);
+  lower4(ucon, g.gcov, ucov);
+  bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
+  for (int j = 1; j <= 3; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[0] * ucon[j]) / ucon[0];
+  lower4(bcon, g.gcov, bcov);
+  return bcon[0] * bcov[0] + bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
+}
+
+// ucon2pr(VELREL4), transforms.c:322-346
+void ucon_to_rel4(const double* ucon, const G& g, double* pr)
+{
+  double alphasq = 1. / (-g.gcon[0]);
+  double gammaoalpha = ucon[0];
+  for (int j = 1; j <= 3; j++) pr[U1 + j - 1] = ucon[j] + alphasq * g.gcon[j] * gammaoalpha;
+}
+
+int limit_gamma(double gammamax, double* pr, const G& g)
+{
+  if (gammamax <= 1.0) return 0;
+  double gamma = gamma_of(pr, g);
+  if (gamma > gammamax && gamma != 1.0) {
+    double pref = (gammamax * gammamax - 1.) / (gamma * gamma - 1.);
+    if (pref < 0.0) return 1;
+    double f = sqrt(pref);
+    pr[U1] *= f;
+    pr[U2] *= f;
+    pr[U3] *= f;
+  }
+  return 0;
+}
+
+// the reference's seeded generator ranc() (ranc.c:31-54) over libc rand()
+struct Ranc {
+  int aa[64], S[64], n = 0;
+  void seed(int iseed)
+  {
+    static const int P[64] = {46337, 46327, 46309, 46307, 46301, 46279, 46273, 46271, 46261, 46237, 46229, 46219, 46199,
+                              46187, 46183, 46181, 46171, 46153, 46147, 46141, 46133, 46103, 46099, 46093, 46091, 46073,
+                              46061, 46051, 46049, 46027, 46021, 45989, 45979, 45971, 45959, 45953, 45949, 45943, 45893,
+                              45887, 45869, 45863, 45853, 45841, 45833, 45827, 45823, 45821, 45817, 45779, 45767, 45763,
+                              45757, 45751, 45737, 45707, 45697, 45691, 45677, 45673, 45667, 45659, 45641, 45631};
+    srand(iseed);
+    n = 0;
+    for (int i = 0; i < 64; i++) {
+      aa[i] = 0;
+      S[i] = 0;
+      while ((aa[i] = (0x7fff & rand())) < (2 << 8) || aa[i] > P[i] - (2 << 8))
+        ;
+      while ((S[i] = (0x7fff & rand())) < 1 || aa[i] > P[i] - 1)
+        ;
+    }
+    memcpy(Pp, P, sizeof(P));
+  }
+  int Pp[64];
+  double next()
+  {
+    n = S[n] & (64 - 1);
+    S[n] = (S[n] * aa[n]) % Pp[n];
+    return (double)S[n] / (double)Pp[n];
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void harm_torus_default_params(harm_torus_params* p)
+{
+  memset(p, 0, sizeof(*p));
+  p->n1 = 128;
+  p->n2 = 128;
+  p->a = 0.9375;
+  p->hslope = 0.3;
+  p->rout = 40.0;
+  p->rin_over_rhor = 0.98;
+  p->gam = 4. / 3.;
+  p->torus_rin = 6.0;
+  p->torus_rmax = 12.0;
+  p->kappa = 1.e-3;
+  p->beta = 1.e2;
+  p->randfact = 4.e-2;
+  p->seed = 7;
+  p->rhomin = 1.e-4;
+  p->uumin = 1.e-6;
+  p->rhominlimit = 1.e-20;
+  p->uuminlimit = 1.e-20;
+  p->gammamax = 25.0;
+}
+
+int harm_torus_geometry(const harm_torus_params* P, double* gcov, double* gcon, double* gdet, double* conn, double* floors,
+                        double* grid_out)
+{
+  if (!P || !gcov || !gcon || !gdet || !conn || !floors) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n1m = n1 + 2 * NG, n2m = n2 + 2 * NG;
+  Coords c;
+  c.a = P->a;
+  c.R0 = 0.0;
+  const double rhor = 1. + 1 * sqrt(1. - c.a * c.a);  // rhor_calc(0), phys.c:1075
+  c.Rin = P->rin_over_rhor * rhor;
+  c.Rout = P->rout;
+  c.hslope = P->hslope;
+  // set_points defcoord 0, coord.c:722-727
+  c.startx1 = log(c.Rin - c.R0);
+  c.startx2 = 0.;
+  c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / n1;
+  c.dx2 = 1. / n2;
+  for (int i = -NG; i < n1 + NG; i++)
+    for (int j = -NG; j < n2 + NG; j++) {
+      const long long zr = (long long)(i + NG) * n2m + (j + NG);
+      for (int loc = 3; loc >= 0; loc--) {
+        double X[4], gv[4][4], gn[4][4];
+        coord_of(c, i, j, loc, X);
+        gcov_prim(c, X, gv);
+        gcon_prim(c, X, gn);
+        memcpy(gcov + (zr * 4 + loc) * 16, gv, sizeof(gv));
+        memcpy(gcon + (zr * 4 + loc) * 16, gn, sizeof(gn));
+        gdet[zr * 4 + loc] = gdet_of(gv);
+        if (loc == CENT) {
+          double cn[4][4][4];
+          conn_of(c, X, gn, cn);
+          memcpy(conn + zr * 64, cn, sizeof(cn));
+          // set_density_floors rescaletype 0 + fixup1zone clamps, fixup.c:996-1110, 295-307
+          double r, th;
+          bl_of(c, X, &r, &th);
+          double fr = P->rhomin * pow(r, -1.5), fu = P->uumin * pow(r, -2.5);
+          if (fr < P->rhominlimit) fr = P->rhominlimit;
+          if (fu < P->uuminlimit) fu = P->uuminlimit;
+          floors[zr * 2 + 0] = fr;
+          floors[zr * 2 + 1] = fu;
+        }
+      }
+    }
+  if (grid_out) {
+    grid_out[0] = c.startx1;
+    grid_out[1] = c.startx2;
+    grid_out[2] = c.dx1;
+    grid_out[3] = c.dx2;
+    grid_out[4] = c.Rin;
+    grid_out[5] = rhor;
+  }
+  (void)n1m;
+  return HARM_OK;
+}
+
+// init() of initbase.c:297-562 with init.fishmon.c's torus, up to (but not
+// including) the final fixup/bound: the caller applies harm_torus_finish()
+// or uploads and lets the device bound it.
+int harm_torus_init(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet, double* prims)
+{
+  if (!P || !gcov || !gcon || !gdet || !prims) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG, n1m = n1 + 2 * NG;
+  Coords c;
+  c.a = P->a;
+  c.R0 = 0.0;
+  const double rhor = 1. + 1 * sqrt(1. - c.a * c.a);
+  c.Rin = P->rin_over_rhor * rhor;
+  c.Rout = P->rout;
+  c.hslope = P->hslope;
+  c.startx1 = log(c.Rin - c.R0);
+  c.startx2 = 0.;
+  c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / n1;
+  c.dx2 = 1. / n2;
+  const double a = c.a, gam = P->gam;
+  auto Z = [&](int i, int j) { return (long long)(i + NG) * n2m + (j + NG); };
+  auto geo = [&](int i, int j) {
+    G g;
+    const long long z = Z(i, j);
+    g.gcov = gcov + (z * 4 + CENT) * 16;
+    g.gcon = gcon + (z * 4 + CENT) * 16;
+    g.g = gdet[z * 4 + CENT];
+    return g;
+  };
+  auto PR = [&](int i, int j) { return prims + Z(i, j) * 8; };
+  memset(prims, 0, sizeof(double) * 8 * (size_t)n1m * n2m);
+
+  Ranc rng;
+  rng.seed(P->seed);
+  rng.next();  // ranc(7) in init_global returns (and consumes) a deviate too
+  // lfish_calc, init.fishmon.c:380-405
+  const double rmax = P->torus_rmax, rin = P->torus_rin;
+  const double r_ = rmax;
+  const double l =
+      (((pow(a, 2) - 2. * a * sqrt(r_) + pow(r_, 2)) *
+        ((-2. * a * r_ * (pow(a, 2) - 2. * a * sqrt(r_) + pow(r_, 2))) / sqrt(2. * a * sqrt(r_) + (-3. + r_) * r_) +
+         ((a + (-2. + r_) * sqrt(r_)) * (pow(r_, 3) + pow(a, 2) * (2. + r_))) / sqrt(1 + (2. * a) / pow(r_, 1.5) - 3. / r_))) /
+       (pow(r_, 3) * sqrt(2. * a * sqrt(r_) + (-3. + r_) * r_) * (pow(a, 2) + (-2. + r_) * r_)));
+  const double kappa = P->kappa;
+  // init_dsandvels over the full grid (i outer), init.fishmon.c:115-226
+  for (int i = -NG; i < n1 + NG; i++)
+    for (int j = -NG; j < n2 + NG; j++) {
+      double X[4], r, th;
+      coord_of(c, i, j, CENT, X);
+      bl_of(c, X, &r, &th);
+      const double sth = sin(th), cth = cos(th);
+      const double DD = r * r - 2. * r + a * a;
+      const double AA = (r * r + a * a) * (r * r + a * a) - DD * a * a * sth * sth;
+      const double SS = r * r + a * a * cth * cth;
+      const double thin = M_PI / 2.;
+      const double sthin = sin(thin), cthin = cos(thin);
+      const double DDin = rin * rin - 2. * rin + a * a;
+      const double AAin = (rin * rin + a * a) * (rin * rin + a * a) - DDin * a * a * sthin * sthin;
+      const double SSin = rin * rin + a * a * cthin * cthin;
+      double lnh;
+      if (r >= rin) {
+        lnh = 0.5 * log((1. + sqrt(1. + 4. * (l * l * SS * SS) * DD / (AA * sth * AA * sth))) / (SS * DD / AA)) -
+              0.5 * sqrt(1. + 4. * (l * l * SS * SS) * DD / (AA * AA * sth * sth)) - 2. * a * r * l / AA -
+              (0.5 * log((1. + sqrt(1. + 4. * (l * l * SSin * SSin) * DDin / (AAin * AAin * sthin * sthin))) /
+                         (SSin * DDin / AAin)) -
+               0.5 * sqrt(1. + 4. * (l * l * SSin * SSin) * DDin / (AAin * AAin * sthin * sthin)) - 2. * a * rin * l / AAin);
+      } else {
+        lnh = 1.;
+      }
+      double* pr = PR(i, j);
+      const G g = geo(i, j);
+      if (lnh < 0. || r < rin) {
+        // set_atmosphere(-1), fixup.c:1121-1190, then the PRIMECOORDS round
+        // trip of bl2met2metp2v (transforms.c:9-47)
+        pr[RHO] = P->rhomin * pow(r, -1.5);
+        pr[UU] = P->uumin * pow(r, -2.5);
+        pr[U1] = pr[U2] = pr[U3] = 0.0;
+        pr[B1] = pr[B2] = pr[B3] = 0;
+        double ucon[4];
+        ucon_rel4(pr, g, ucon);
+        ucon_to_rel4(ucon, g, pr);
+      } else {
+        const double hm1 = exp(lnh) - 1.;
+        const double rho = pow(hm1 * (gam - 1.) / (kappa * gam), 1. / (gam - 1.));
+        const double u = kappa * pow(rho, gam) / (gam - 1.);
+        const double expm2chi = SS * SS * DD / (AA * AA * sth * sth);
+        const double up1 = sqrt((-1. + sqrt(1. + 4. * l * l * expm2chi)) / 2.);
+        const double up = 2. * a * r * sqrt(1. + up1 * up1) / sqrt(AA * SS * DD) + sqrt(SS / AA) * up1 / sth;
+        pr[RHO] = rho;
+        pr[UU] = u * (1. + P->randfact * (rng.next() - 0.5));
+        pr[U1] = 0.;
+        pr[U2] = 0.;
+        pr[U3] = 1.0 * up;
+        // VEL4 in Boyer-Lindquist -> u^mu (ucon_calc_4vel with the BL metric,
+        // metric.c:601-655, phys.c:962-1012) -> Kerr-Schild (bltoks,
+        // transforms.c:109-166) -> prime coords (mettometp) -> rel. 4-velocity
+        double ucon[4];
+        {
+          const double s2 = sth * sth, a2 = a * a, r2 = r * r;
+          const double DDb = 1. - 2. / r + a2 / r2;
+          const double mu = 1. + a2 * cth * cth / r2;
+          double bl[4][4] = {{0}};
+          bl[0][0] = (-(1. - 2. / (r * mu)));
+          bl[0][3] = (-2. * a * s2 / (r * mu));
+          bl[1][1] = (mu / DDb);
+          bl[2][2] = (r2 * mu);
+          bl[3][0] = bl[0][3];
+          bl[3][3] = (r2 * sth * sth * (1. + a2 / r2 + 2. * a2 * s2 / (r2 * r * mu)));
+          ucon[1] = pr[U1];
+          ucon[2] = pr[U2];
+          ucon[3] = pr[U3];
+          const double AAq = bl[0][0];
+          const double BBq = 2. * (bl[0][1] * ucon[1] + bl[0][2] * ucon[2] + bl[0][3] * ucon[3]);
+          const double CCq = 1. + bl[1][1] * ucon[1] * ucon[1] + bl[2][2] * ucon[2] * ucon[2] + bl[3][3] * ucon[3] * ucon[3] +
+                             2. * (bl[1][2] * ucon[1] * ucon[2] + bl[1][3] * ucon[1] * ucon[3] + bl[2][3] * ucon[2] * ucon[3]);
+          const double discr = BBq * BBq - 4. * AAq * CCq;
+          if (discr < 0.) return HARM_EINVAL;
+          ucon[0] = (-BBq - sqrt(discr)) / (2. * AAq);
+        }
+        {
+          double tr[4][4] = {{0}};
+          tr[0][0] = (1);
+          tr[0][1] = (2. * r / (r * r - 2. * r + a * a));
+          tr[1][1] = (1);
+          tr[2][2] = (1);
+          tr[3][1] = (a / (r * r - 2. * r + a * a));
+          tr[3][3] = (1);
+          double t[4] = {0., 0., 0., 0.};
+          for (int jj = 0; jj < 4; jj++)
+            for (int kk = 0; kk < 4; kk++) t[jj] += tr[jj][kk] * ucon[kk];
+          for (int jj = 0; jj < 4; jj++) ucon[jj] = t[jj];
+        }
+        {
+          double d[4];
+          dxdxp_of(c, X, r, d);
+          double id[4][4] = {{0}};
+          for (int k = 0; k < 4; k++) id[k][k] = 1.0 / d[k];
+          double t[4] = {0., 0., 0., 0.};
+          for (int jj = 0; jj < 4; jj++)
+            for (int kk = 0; kk < 4; kk++) t[jj] += id[jj][kk] * ucon[kk];
+          for (int jj = 0; jj < 4; jj++) ucon[jj] = t[jj];
+        }
+        ucon_to_rel4(ucon, g, pr);
+      }
+    }
+  // normalize_densities, init.fishmon.c:278-306
+  double rhomax = 0, umax = 0;
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      double X[4], r, th;
+      coord_of(c, i, j, CENT, X);
+      bl_of(c, X, &r, &th);
+      const double* pr = PR(i, j);
+      if (pr[RHO] > rhomax) rhomax = pr[RHO];
+      if (pr[UU] > umax && r > rin) umax = pr[UU];
+    }
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      PR(i, j)[RHO] /= rhomax;
+      PR(i, j)[UU] /= rhomax;
+    }
+  umax /= rhomax;
+  rhomax = 1.;
+  // init_atmosphere on the active zones, init.fishmon.c:90-112: where the
+  // torus is below the atmosphere, take the atmosphere (the reference's
+  // uninitialised B components of its temporary are taken as zero here)
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      double X[4], r, th;
+      coord_of(c, i, j, CENT, X);
+      bl_of(c, X, &r, &th);
+      double* pr = PR(i, j);
+      const G g = geo(i, j);
+      const double arho = P->rhomin * pow(r, -1.5), au = P->uumin * pow(r, -2.5);
+      if (pr[RHO] < arho) {
+        pr[RHO] = arho;
+        pr[UU] = au;
+        pr[U1] = pr[U2] = pr[U3] = 0.0;
+        pr[B1] = pr[B2] = pr[B3] = 0.0;
+      }
+      double ucon[4];
+      ucon_rel4(pr, g, ucon);
+      ucon_to_rel4(ucon, g, pr);
+    }
+  // fixup(): fixup1zone on the active zones (floors, gamma limit)
+  const double gmax = P->gammamax;
+  auto fixup_all = [&]() {
+    for (int i = 0; i < n1; i++)
+      for (int j = 0; j < n2; j++) {
+        double X[4], r, th;
+        coord_of(c, i, j, CENT, X);
+        bl_of(c, X, &r, &th);
+        double* pr = PR(i, j);
+        double fr = P->rhomin * pow(r, -1.5), fu = P->uumin * pow(r, -2.5);
+        if (fr < P->rhominlimit) fr = P->rhominlimit;
+        if (fu < P->uuminlimit) fu = P->uuminlimit;
+        if (fr > pr[RHO]) pr[RHO] = fr;
+        if (fu > pr[UU]) pr[UU] = fu;
+        limit_gamma(gmax, pr, geo(i, j));
+      }
+  };
+  fixup_all();
+  // the vector potential only needs bounded densities: rho is a plain copy
+  // in bound_prim (outflow in x1, mirror in x2)
+  for (int j = 0; j < n2; j++)
+    for (int i = -1; i >= -NG; i--) {
+      PR(i, j)[RHO] = PR(0, j)[RHO];
+      PR(n1 - 1 - i, j)[RHO] = PR(n1 - 1, j)[RHO];
+    }
+  for (int i = -NG; i < n1 + NG; i++)
+    for (int j = -NG; j <= -1; j++) {
+      PR(i, j)[RHO] = PR(i, -j - 1)[RHO];
+      PR(i, n2 - 1 - j)[RHO] = PR(i, n2 + j)[RHO];
+    }
+  // init_vpot at corners (DISKFIELD), init.fishmon.c:236-268, and
+  // vpot2field, initbase.c:565-618, on the active zones
+  std::vector<double> A((size_t)(n1 + 1) * (n2 + 1), 0.0);
+  for (int i = 0; i <= n1; i++)
+    for (int j = 0; j <= n2; j++) {
+      double rho_av = 0.25 * (PR(i, j)[RHO] + PR(i - 1, j)[RHO] + PR(i, j - 1)[RHO] + PR(i - 1, j - 1)[RHO]);
+      double q = rho_av / rhomax - 0.2;
+      double Av = 0;
+      if (q > 0.) Av += q;
+      A[(size_t)i * (n2 + 1) + j] = Av;
+    }
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      const G g = geo(i, j);
+      auto AA_ = [&](int ii, int jj) { return A[(size_t)ii * (n2 + 1) + jj]; };
+      double* pr = PR(i, j);
+      pr[B1] = (-AA_(i, j) + AA_(i, j + 1) - AA_(i + 1, j) + AA_(i + 1, j + 1)) / (2. * c.dx2 * g.g);
+      pr[B2] = -(-AA_(i, j) - AA_(i, j + 1) + AA_(i + 1, j) + AA_(i + 1, j + 1)) / (2. * c.dx1 * g.g);
+    }
+  // normalize_field twice, init.fishmon.c:310-375 (initbase.c:459 and 490)
+  for (int pass = 0; pass < 2; pass++) {
+    double bsq_max = 0.;
+    for (int i = 0; i < n1; i++)
+      for (int j = 0; j < n2; j++) {
+        double b = bsq_of(PR(i, j), geo(i, j));
+        if (b > bsq_max) bsq_max = b;
+      }
+    const double beta_act = (gam - 1.) * umax / (0.5 * bsq_max);
+    const double norm = sqrt(beta_act / P->beta);
+    for (int i = 0; i < n1; i++)
+      for (int j = 0; j < n2; j++) {
+        PR(i, j)[B1] *= norm;
+        PR(i, j)[B2] *= norm;
+        PR(i, j)[B3] *= norm;
+      }
+  }
+  fixup_all();
+  return HARM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+/*
+ * harm_b200.h -- C ABI of the B200 (sm_100a) implementation of HARM's
+ * per-step finite-volume update.
+ *
+ * This is the drop-in boundary for the reference's
+ *     int step_ch(void)                        (step_ch.c:16, global.h:1383)
+ * which reads and writes the reference's globals p, pk, pflag, dt, t,
+ * realnstep and the geometry tables gcov/gcon/gdet/conn (defs.h:4-309).
+ * A host shim that replaces step_ch() calls harm_step() on a context that
+ * holds device-resident copies of those arrays.
+ *
+ * Array arguments use the reference's own memory layout (defs.h) over the
+ * full grid including NG = 3 ghost zones per side, n1m = n1 + 6 rows of
+ * n2m = n2 + 6 zones, x2 index fastest:
+ *   prims   [n1m][n2m][8]            rho, u, u~1, u~2, u~3, B1, B2, B3
+ *   pflag   [n1m][n2m][5]            pflag[..][0] = FLAGUTOPRIMFAIL,
+ *                                    [2] = FLAGBSQORHO, [3] = FLAGBSQOU
+ *   gcov    [n1m][n2m][4][4][4]      [loc][mu][nu], loc = FACE1, FACE2,
+ *   gcon    [n1m][n2m][4][4][4]      CORN, CENT (global.h:645-648)
+ *   gdet    [n1m][n2m][4]
+ *   conn    [n1m][n2m][4][4][4]      conn[k][l][j] = Gamma^k_{l j}
+ *   floors  [n1m][n2m][2]            rho and u floors at CENT, already
+ *                                    clamped below by RHOMINLIMIT/UUMINLIMIT
+ *                                    (fixup.c:295-307)
+ *
+ * Every entry point returns 0 on success or a positive HARM_E* code; no
+ * entry point aborts the process.  One context = one CUDA stream = one host
+ * thread.  There is no CPU fallback: without a usable CUDA device
+ * harm_create() fails with HARM_ENODEVICE.
+ */
+#ifndef HARM_B200_H
+#define HARM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define HARM_OK 0
+#define HARM_EINVAL 1        /* invalid argument or configuration */
+#define HARM_ENODEVICE 2     /* no CUDA device / not sm_100 */
+#define HARM_ECUDA 3         /* CUDA runtime error */
+#define HARM_ENOMEM 4        /* device allocation failed */
+#define HARM_EGEOMETRY 5     /* geometry tables not symmetric or not uploaded */
+#define HARM_EFAIL 6         /* the step hit a fatal check of the reference
+                                (fail() codes, global.h:562-579); see
+                                harm_status.fail_code */
+
+/* limiter / Riemann solver / equations of motion (step_ch.h:22-80) */
+#define HARM_LIM_MC 3
+#define HARM_LIM_PARA 4
+#define HARM_FLUX_LAXF 0
+#define HARM_FLUX_HLL 1
+#define HARM_EOM_GRMHD 0
+
+/* Run-time knobs of the reference (initbase.c:119-243 and the problem's
+   init_global), plus the grid size that the reference fixes at compile time
+   (global.h:126-127). */
+typedef struct harm_config {
+  int n1, n2;           /* interior zones */
+  int lim;              /* HARM_LIM_MC or HARM_LIM_PARA */
+  int fluxmethod;       /* HARM_FLUX_HLL or HARM_FLUX_LAXF */
+  int eom;              /* HARM_EOM_GRMHD */
+  int reserved;         /* must be 0 */
+  double cour;          /* Courant factor */
+  double gam;           /* adiabatic index */
+  double dx1, dx2;      /* uniform coordinate spacings dx[1], dx[2] */
+  double safe;          /* SAFE: max dt growth per step */
+  double defcon;
+  double gammamax;      /* GAMMAMAX */
+  double gammafail;     /* GAMMAFAIL */
+  double bsqorholimit;  /* BSQORHOLIMIT */
+  double bsqoulimit;    /* BSQOULIMIT */
+  double tf;            /* end time: dt is clamped so that t + dt <= tf */
+} harm_config;
+
+typedef struct harm_status {
+  int fail_code;                 /* reference fail() code, 0 if none */
+  int fail_i, fail_j;            /* zone of the first fatal check */
+  int fixups;                    /* zones repaired by fixup_utoprim, last step */
+  long long realnstep;
+  double t, dt;                  /* time and the next step's dt */
+  unsigned long long newton_iters; /* Newton iterations since harm_set_time */
+} harm_status;
+
+typedef struct harm_ctx harm_ctx;
+
+/* Allocates the device state for cfg on `stream` (a cudaStream_t, or NULL
+   for the default stream). */
+int harm_create(const harm_config* cfg, void* stream, harm_ctx** out);
+
+/* Uploads the geometry tables computed by set_grid() (set_grid.c:6-89) and
+   the per-zone floors; once, before the first step. */
+int harm_upload_geometry(harm_ctx* ctx, const double* gcov, const double* gcon, const double* gdet,
+                         const double* conn, const double* floors);
+
+/* Host -> device copy of p (and pflag, may be NULL) from the reference
+   layout; also resets the device copy of fixup_checksolution's gammacheck
+   table when reset_gammacheck != 0 (fixup.c:393 keeps it static). */
+int harm_set_prims(harm_ctx* ctx, const double* prims, const int* pflag, int reset_gammacheck);
+
+/* Device -> host copy of p and pflag (either may be NULL). */
+int harm_get_prims(harm_ctx* ctx, double* prims, int* pflag);
+
+/* Fills the ghost zones of the device state as bound_prim() does
+   (bounds.fishmon.c:14-330), e.g. after uploading an unbounded state. */
+int harm_bound_prims(harm_ctx* ctx);
+
+/* Sets t, dt and realnstep (as init() or a restart leaves them). */
+int harm_set_time(harm_ctx* ctx, double t, double dt, long long realnstep);
+
+/* Enqueues nsteps full steps of step_ch() on the context's stream
+   (asynchronous; the first call captures a CUDA graph of one step). */
+int harm_step(harm_ctx* ctx, int nsteps);
+
+/* Waits for the stream and reports the run state; returns HARM_EFAIL when a
+   fatal check fired. */
+int harm_sync(harm_ctx* ctx, harm_status* st);
+
+/* Host copies of the last substep's F1, F2 after fix_flux and flux-CT, in
+   the reference layout [n1m][n2m][8] (what diag_flux() reads). */
+int harm_get_fluxes(harm_ctx* ctx, double* F1, double* F2);
+
+/* Diagnostics: runs one step outside the graph with a CUDA event after
+   every kernel and returns, per kernel class (harm_kernel_name(k), k <
+   HARM_NKERNELS), the summed device time in ms and the launch count. */
+#define HARM_NKERNELS 12
+int harm_profile_step(harm_ctx* ctx, double* ms, int* launches, int nclasses);
+const char* harm_kernel_name(int k);
+
+void harm_destroy(harm_ctx* ctx);
+
+const char* harm_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,55 @@
+/*
+ * harm_setup.h -- host-side problem set-up for standalone runs: the grid
+ * geometry and the Fishbone-Moncrief torus of the reference's plugin
+ * surface (coord.c, metric.c, set_grid.c, init.fishmon.c, initbase.c).
+ *
+ * A drop-in host keeps calling the reference's own set_grid()/init(); these
+ * entry points exist so that the library can produce the same inputs without
+ * the reference.  All arrays use the reference layout described in
+ * harm_b200.h.
+ */
+#ifndef HARM_SETUP_H
+#define HARM_SETUP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct harm_torus_params {
+  int n1, n2;             /* interior zones */
+  int seed;               /* ranc() seed of init_global (init.fishmon.c:64) */
+  int reserved;
+  double a;               /* black-hole spin (init.fishmon.c:40) */
+  double hslope;          /* MKS theta concentration (defcoord 0) */
+  double rout;            /* outer radius */
+  double rin_over_rhor;   /* Rin = rin_over_rhor * r_horizon */
+  double gam;             /* adiabatic index */
+  double torus_rin, torus_rmax, kappa, beta, randfact;  /* init.fishmon.c:134-139 */
+  double rhomin, uumin;   /* floor coefficients, rho >= rhomin r^-1.5, u >= uumin r^-2.5 */
+  double rhominlimit, uuminlimit;
+  double gammamax;
+} harm_torus_params;
+
+/* The benchmark torus: a = 0.9375, hslope 0.3, Rout 40, Rin = 0.98 r_h,
+   rin 6, rmax 12, kappa 1e-3, beta 100, 4% seeded u perturbation (seed 7),
+   gamma 4/3, floors 1e-4 r^-1.5 / 1e-6 r^-2.5, GAMMAMAX 25, 128 x 128. */
+void harm_torus_default_params(harm_torus_params* p);
+
+/* set_grid() (set_grid.c:6-89) for MKS defcoord 0 on Kerr-Schild: gcov,
+   gcon, gdet at the four grid locations, the numerical connection at CENT
+   (metric.c:1188-1262) and the per-zone floors.  grid_out (may be NULL)
+   receives startx1, startx2, dx1, dx2, Rin, r_horizon. */
+int harm_torus_geometry(const harm_torus_params* p, double* gcov, double* gcon, double* gdet, double* conn,
+                        double* floors, double* grid_out);
+
+/* init()'s fresh start (initbase.c:297-562) with the torus of
+   init.fishmon.c, given the geometry from harm_torus_geometry().  Active
+   zones are final; ghost zones still need bound_prim (harm_bound_prims()
+   on the device, after harm_set_prims()). */
+int harm_torus_init(const harm_torus_params* p, const double* gcov, const double* gcon, const double* gdet,
+                    double* prims);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

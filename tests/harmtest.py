@@ -1,0 +1,201 @@
+"""Test support: the oracle (C restatement, oracle/harm_oracle.c), the
+reference compiled from its own sources (oracle/_ref, optional) and helpers
+to drive them on the same inputs as the GPU path.
+
+The oracle is test infrastructure only; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SRC = os.path.join(ORACLE_DIR, "harm_oracle.c")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "libharm_oracle.so")
+REF_DIR = os.path.join(ORACLE_DIR, "_ref")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+NG = 3
+
+
+class OracleConfig(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("lim", ctypes.c_int), ("fluxmethod", ctypes.c_int),
+                ("eom", ctypes.c_int), ("cour", ctypes.c_double), ("gam", ctypes.c_double), ("dx1", ctypes.c_double),
+                ("dx2", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
+                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double)]
+
+
+def build_oracle(force=False):
+    """Compiles the C restatement with no FP contraction (like the reference)."""
+    if (not force and os.path.exists(ORACLE_LIB)
+            and os.path.getmtime(ORACLE_LIB) >= os.path.getmtime(ORACLE_SRC)
+            and os.path.getmtime(ORACLE_LIB) >= os.path.getmtime(os.path.join(ORACLE_DIR, "harm_oracle.h"))):
+        return ORACLE_LIB
+    tmp = ORACLE_LIB + ".tmp%d" % os.getpid()
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-o", tmp, ORACLE_SRC,
+                    "-lm"], check=True)
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+_oracle = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        lib = ctypes.CDLL(build_oracle())
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        lib.ho_create.restype = vp
+        lib.ho_create.argtypes = [ctypes.POINTER(OracleConfig), dp, dp, dp, dp, dp]
+        lib.ho_destroy.argtypes = [vp]
+        lib.ho_step.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), dp, dp]
+        lib.ho_bound.argtypes = [vp, dp]
+        lib.ho_bsqflags.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
+        lib.ho_get_fluxes.argtypes = [vp, dp, dp]
+        lib.ho_ncyclebreak.argtypes = [vp]
+        lib.ho_ncyclebreak.restype = ctypes.c_long
+        lib.ho_cycle_break_uniform.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        lib.ho_cycle_break_uniform.restype = ctypes.c_double
+        _oracle = lib
+    return _oracle
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    """The C restatement run on given geometry and state."""
+
+    def __init__(self, n1, n2, geom, *, lim=3, fluxmethod=1, cour=0.8, gam=4.0 / 3.0, dx1, dx2, safe=1.3,
+                 defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1e30):
+        self.lib = oracle_lib()
+        self.cfg = OracleConfig(n1, n2, lim, fluxmethod, 0, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+                                bsqorholimit, bsqoulimit, tf)
+        self.geom = {k: np.ascontiguousarray(geom[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "conn",
+                                                                                     "floors")}
+        g = self.geom
+        self.h = self.lib.ho_create(ctypes.byref(self.cfg), _dp(g["gcov"]), _dp(g["gcon"]), _dp(g["gdet"]),
+                                    _dp(g["conn"]), _dp(g["floors"]))
+        self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ho_destroy(self.h)
+            self.h = None
+
+    def bound(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float64).copy()
+        self.lib.ho_bound(self.h, _dp(p))
+        return p
+
+    def step(self, p, pflag, t, dt):
+        """one step in place; returns (rc, t, dt)"""
+        tt, dd = ctypes.c_double(t), ctypes.c_double(dt)
+        rc = self.lib.ho_step(self.h, _dp(p), pflag.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(tt),
+                              ctypes.byref(dd))
+        return rc, tt.value, dd.value
+
+    def fluxes(self):
+        f1 = np.zeros((self.n1m, self.n2m, 8))
+        f2 = np.zeros((self.n1m, self.n2m, 8))
+        self.lib.ho_get_fluxes(self.h, _dp(f1), _dp(f2))
+        return f1, f2
+
+    def ncyclebreak(self):
+        return self.lib.ho_ncyclebreak(self.h)
+
+
+# ---------------------------------------------------------------- reference
+def ref_lib_path(n1, n2, problem="torus"):
+    p = os.path.join(REF_DIR, f"libharmref_{problem}_{n1}x{n2}.so")
+    return p if os.path.exists(p) else None
+
+
+def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
+    """Runs in a child process: reference init + nsteps steps, pickled to outpath."""
+    import pickle
+    lib = ctypes.CDLL(libpath)
+    lib.hr_configure.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double]
+    lib.hr_get_ncyclebreak.restype = ctypes.c_long
+    lib.hr_configure(lim, flux, 2, cour, 0, 1e30)
+    work = tempfile.mkdtemp(prefix="harmref_")
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(2)
+    os.dup2(devnull, 2)
+    os.dup2(devnull, 1)
+    rc = lib.hr_init(work.encode())
+    os.dup2(saved, 2)
+    if rc != 0:
+        raise RuntimeError("reference init failed")
+    n1, n2 = lib.hr_n1(), lib.hr_n2()
+    m1, m2 = n1 + 2 * NG, n2 + 2 * NG
+    V = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    s = np.zeros(32)
+    lib.hr_get_scalars(V(s))
+    geom = dict(gcov=np.zeros((m1, m2, 4, 4, 4)), gcon=np.zeros((m1, m2, 4, 4, 4)), gdet=np.zeros((m1, m2, 4)),
+                conn=np.zeros((m1, m2, 4, 4, 4)), floors=np.zeros((m1, m2, 2)))
+    lib.hr_get_geometry(V(geom["gcov"]), V(geom["gcon"]), V(geom["gdet"]), V(geom["conn"]))
+    lib.hr_get_floors(V(geom["floors"]))
+    scal0 = s.copy()
+    ps, pfs, ts = [], [], []
+    for n in range(nsteps + 1):
+        p = np.zeros((m1, m2, 8))
+        pf = np.zeros((m1, m2, 5), dtype=np.int32)
+        lib.hr_get_prims(V(p))
+        lib.hr_get_pflag(V(pf))
+        lib.hr_get_scalars(V(s))
+        ps.append(p)
+        pfs.append(pf)
+        ts.append((s[0], s[1]))
+        if n < nsteps:
+            os.dup2(devnull, 2)
+            rcs = lib.hr_step(1)
+            os.dup2(saved, 2)
+            if rcs != 0:
+                raise RuntimeError("reference step failed")
+    f1 = np.zeros((m1, m2, 8))
+    f2 = np.zeros((m1, m2, 8))
+    lib.hr_get_fluxes(V(f1), V(f2))
+    with open(outpath, "wb") as f:
+        pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, F1=f1, F2=f2,
+                         ncyclebreak=lib.hr_get_ncyclebreak()), f, protocol=4)
+
+
+def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800):
+    """Runs the compiled reference (init + nsteps steps) in a fresh child
+    process (its init() can run once per process) and returns its arrays."""
+    import pickle
+    import sys
+    path = ref_lib_path(n1, n2, problem)
+    if path is None:
+        return None
+    fd, out = tempfile.mkstemp(suffix=".pkl", prefix="harmref_")
+    os.close(fd)
+    code = ("import sys; sys.path.insert(0, %r); import harmtest; harmtest._ref_worker(%r, %d, %d, %r, %d, %r)"
+            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, float(cour), nsteps, out))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed (rc=%d): %s" % (r.returncode, r.stderr[-2000:]))
+        with open(out, "rb") as f:
+            return pickle.load(f)
+    finally:
+        os.unlink(out)
+
+
+def ref_config(r):
+    """harm config keyword arguments from a reference run's scalars."""
+    s = r["scalars"]
+    return dict(cour=s[12], gam=s[3], dx1=s[10], dx2=s[11], safe=s[20], defcon=s[21], gammamax=s[16],
+                gammafail=s[17], bsqorholimit=s[18], bsqoulimit=s[19])
+
+
+def interior(a):
+    return a[NG:-NG, NG:-NG]
