@@ -495,3 +495,92 @@ int harm_get_fluxes(harm_ctx* c, double* F1, double* F2)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free step (harm_step_noalloc in include/harm_b200.h).
+//
+// For callers that cannot call cudaMalloc: the scratch of one step lives in
+// this file-scope device array, so the call allocates nothing.  Every device
+// that loads the library holds one copy of it until the process exits.
+static constexpr long long NOALLOC_MAX_PLANE = 5632;  // pitch * (n2 + 6): 64 x 64 interior zones fit
+static constexpr int NOALLOC_MAX_BLOCKS = 256;        // x1/x2 flux blocks of 32 x 4 zones
+static constexpr long long NA_DPLANES = 31;           // pk0 8, F1 8, F2 8, emf, gammacheck, fixbuf 5
+static constexpr long long NA_OFF_BLOCKMIN = NA_DPLANES * NOALLOC_MAX_PLANE;
+static constexpr long long NA_OFF_SCALARS = NA_OFF_BLOCKMIN + 2 * NOALLOC_MAX_BLOCKS;
+static constexpr long long NA_OFF_BYTES = NA_OFF_SCALARS + 32;  // 256 B for DevScalars
+static constexpr long long NA_DOUBLES = NA_OFF_BYTES + (3 * NOALLOC_MAX_PLANE) / 8 + 32;
+static_assert(sizeof(DevScalars) <= 32 * sizeof(double), "DevScalars must fit its slot");
+static __device__ __align__(256) double g_noalloc_scratch[NA_DOUBLES];
+
+static double* g_noalloc_addr[64];  // per device: address of g_noalloc_scratch
+
+extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, double* d_prims, int* d_pflag, double* t,
+                                 double* dt, int reset_gammacheck, void* stream)
+{
+  if (!cfg || !d_geo || !d_prims || !d_pflag || !t || !dt) return HARM_EINVAL;
+  if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->reserved != 0 || cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
+  if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
+  if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
+  harm_ctx c;
+  memset(&c, 0, sizeof(c));
+  c.cfg = *cfg;
+  c.stream = (cudaStream_t)stream;
+  c.n1m = cfg->n1 + 2 * NG;
+  c.n2m = cfg->n2 + 2 * NG;
+  c.gr.n1 = cfg->n1;
+  c.gr.n2 = cfg->n2;
+  c.gr.pitch = ((c.n1m + 15) / 16) * 16;
+  c.gr.rows = c.n2m;
+  c.gr.plane = (long long)c.gr.pitch * c.gr.rows;
+  const dim3 b(32, 4);
+  const dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, b);
+  c.nblocks_flux = gf.x * gf.y;
+  if (c.gr.plane > NOALLOC_MAX_PLANE || c.nblocks_flux > NOALLOC_MAX_BLOCKS) {
+    fprintf(stderr,
+            "harm_step_noalloc: a %d x %d grid needs %lld doubles per plane; the static scratch holds %lld "
+            "(at most 64 x 64 active zones)\n",
+            cfg->n1, cfg->n2, c.gr.plane, NOALLOC_MAX_PLANE);
+    return HARM_EINVAL;
+  }
+  // set-up, once per device, with that device current: the host-side name of
+  // the array is not a device address
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return HARM_ENODEVICE;
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = (double*)p;
+  }
+  double* s = g_noalloc_addr[dev];
+  const long long pl = c.gr.plane;
+  c.d_p = d_prims;
+  c.d_pflag = d_pflag;
+  c.d_geo = const_cast<double*>(d_geo);
+  c.d_pk0 = s;
+  c.d_F1 = s + 8 * pl;
+  c.d_F2 = s + 16 * pl;
+  c.d_emf = s + 24 * pl;
+  c.d_gammacheck = s + 25 * pl;
+  c.d_fixbuf = s + 26 * pl;
+  c.d_blockmin = s + NA_OFF_BLOCKMIN;
+  c.d_sc = (DevScalars*)(s + NA_OFF_SCALARS);
+  c.d_bsqf = (unsigned char*)(s + NA_OFF_BYTES);
+  c.d_chk = c.d_bsqf + pl;
+  c.geo_ok = true;
+  // the array keeps the last call's contents: the run scalars start from
+  // zero on every call, the check-solution gamma table only when asked
+  DevScalars h;
+  memset(&h, 0, sizeof(h));
+  h.t = *t;
+  h.dt = *dt;
+  CK(cudaMemcpyAsync(c.d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c.stream));
+  if (reset_gammacheck) CK(cudaMemsetAsync(c.d_gammacheck, 0, (size_t)pl * sizeof(double), c.stream));
+  int rc = enqueue_step(&c);
+  if (rc != HARM_OK) return rc;
+  CK(cudaMemcpyAsync(&h, c.d_sc, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  *t = h.t;
+  *dt = h.dt;
+  return h.status ? HARM_EFAIL : HARM_OK;
+}

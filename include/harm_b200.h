@@ -128,6 +128,31 @@ int harm_get_fluxes(harm_ctx* ctx, double* F1, double* F2);
 int harm_profile_step(harm_ctx* ctx, double* ms, int* launches, int nclasses);
 const char* harm_kernel_name(int k);
 
+/* One step of step_ch() that allocates nothing -- no counterpart in the
+   reference.  For callers that cannot call cudaMalloc (a host code that owns
+   all device memory through its own pool, or that runs where allocation is
+   forbidden): the caller passes its own device buffers and the scratch of
+   the step lives in a static array compiled into this library (about 1.4 MB
+   per device, held until the process exits).  Limit: pitch * (n2 + 6) <=
+   5632 doubles per plane, i.e. at most 64 x 64 active zones; larger grids
+   are rejected with HARM_EINVAL and a message on stderr.
+   Inputs/outputs are device arrays in the step's structure-of-arrays layout:
+   a plane holds zone (i, j), i in [-3, n1+3), j in [-3, n2+3), at
+   (j+3)*pitch + (i+3) with pitch = n1+6 rounded up to a multiple of 16;
+   d_prims = 8 planes (rho, u, u~1..3, B1..3), bounded, updated in place;
+   d_pflag = 1 int plane (FLAGUTOPRIMFAIL), updated; d_geo = 126 planes:
+   for loc = FACE1, FACE2, CORN, CENT 10 gcov + 10 gcon (packed symmetric,
+   00 01 02 03 11 12 13 22 23 33) + gdet, then 40 connection planes
+   Gamma^k_{(lj)} (k*10 + packed (l,j)), then the rho and u floors.
+   t and dt are host values, advanced as step_ch() does.  The first call on
+   a device looks up the array's device address (cudaGetSymbolAddress), so
+   make it before any stream capture.  Every call shares the one array:
+   calls that overlap on the GPU race.  The fixup_checksolution gamma table
+   (static in the reference, fixup.c:393) carries over between calls unless
+   reset_gammacheck != 0. */
+int harm_step_noalloc(const harm_config* cfg, const double* d_geo, double* d_prims, int* d_pflag, double* t,
+                      double* dt, int reset_gammacheck, void* stream);
+
 void harm_destroy(harm_ctx* ctx);
 
 const char* harm_error_string(int code);
