@@ -36,14 +36,18 @@ BYTES_PER_ZONE_CYCLE = 2032  # algorithmic FP64 bytes per zone-cycle (see DESIGN
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--lim", default="para", choices=["para", "mc"])
     ap.add_argument("--flux", default="hll", choices=["hll", "laxf"])
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--evolve", type=int, default=400,
+                    help="untimed steps from init before warm-up, so that the timed steps see a developed flow")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=100.0,
+                    help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
 
 
@@ -57,49 +61,48 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled every few ms during the timed
+    region (NVML; nvidia-smi's CSV query as the fallback)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.out = None
+    def __init__(self, gpu_index, period_s=0.002):
+        self.gpu, self.period = gpu_index, period_s
+        self.samples, self.reasons = [], set()
+        self.smax = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self, nv, h):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, bit in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def start(self):
         try:
-            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
-                                         stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._t = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+            self._t.start()
         except Exception:
-            self.proc = None
+            self._t = None
 
     def stop(self):
-        if self.proc is None:
+        if self._t is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.out.flush()
-        self.out.seek(0)
-        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
-        os.unlink(self.out.name)
-        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            if len(r) > 8:
-                for k, nm in enumerate(names):
-                    if r[5 + k].strip().lower() == "active":
-                        reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+        self._stop.set()
+        self._t.join()
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 # ------------------------------------------------------------------ reference
@@ -111,27 +114,30 @@ def _ref_lib(n):
 REF_WORKER = r"""
 import ctypes, os, sys, time, tempfile
 lib = ctypes.CDLL(sys.argv[1])
-lim, nsteps = int(sys.argv[2]), int(sys.argv[3])
+lim, nsteps, budget = int(sys.argv[2]), int(sys.argv[3]), float(sys.argv[5])
 lib.hr_configure.argtypes = [ctypes.c_int]*3 + [ctypes.c_double, ctypes.c_int, ctypes.c_double]
 lib.hr_configure(lim, int(sys.argv[4]), 2, 0.8, 0, 1e30)
 w = tempfile.mkdtemp(prefix="harmref_")
 fd = os.open(os.devnull, os.O_WRONLY); sv = os.dup(1); os.dup2(fd, 1); os.dup2(fd, 2)
 lib.hr_init(w.encode())
 ts = []
+tstart = time.perf_counter()
 for k in range(nsteps):
     t0 = time.perf_counter(); rc = lib.hr_step(1); ts.append(time.perf_counter() - t0)
     if rc: break
+    if k >= 1 and time.perf_counter() - tstart > budget: break
 os.write(sv, (" ".join("%.6f" % t for t in ts) + "\n").encode())
 """
 
 
-def run_reference_procs(n, lim, flux, nsteps, nprocs):
+def run_reference_procs(n, lim, flux, nsteps, nprocs, budget_s=1e9):
     """nprocs independent reference processes (one torus each); per-step wall
-    times of each.  Returns a list of lists."""
+    times of each (a process stops early once budget_s of stepping is spent).
+    Returns a list of lists."""
     lib = _ref_lib(n)
     if lib is None:
         return None
-    procs = [subprocess.Popen([sys.executable, "-c", REF_WORKER, lib, str(lim), str(nsteps), str(flux)],
+    procs = [subprocess.Popen([sys.executable, "-c", REF_WORKER, lib, str(lim), str(nsteps), str(flux), str(budget_s)],
                               stdout=subprocess.PIPE, stderr=subprocess.DEVNULL) for _ in range(nprocs)]
     out = []
     for p in procs:
@@ -165,22 +171,27 @@ def reference_arm(a):
         return 0
     nprocs = max(1, min(cpu_cores(), 16))
     t0 = time.time()
-    per = run_reference_procs(n, lim, flux, a.warmup + a.steps, nprocs)
-    per = [p for p in per if len(p) == a.warmup + a.steps]
+    # a reference step of this torus takes seconds per core: warm-up and the
+    # timed steps are bounded by a wall budget so the run ends in minutes
+    warm = min(a.warmup, 2)
+    per = run_reference_procs(n, lim, flux, warm + a.steps, nprocs, budget_s=a.ref_budget)
+    per = [p for p in per if len(p) > warm]
     if not per:
         print(json.dumps({"impl": "reference", "unavailable": "reference step failed"}))
         return 0
+    ktimed = min(len(p) for p in per) - warm
     # aggregate: all processes advance concurrently; a timed step is the
     # slowest process's step
-    step_times = [max(p[a.warmup + k] for p in per) for k in range(a.steps)]
+    step_times = [max(p[warm + k] for p in per) for k in range(ktimed)]
     tstep = sum(step_times) / len(step_times)
     value = len(per) * n * n / tstep
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": ktimed, "warmup": warm,
+            "steps_requested": a.steps, "warmup_requested": a.warmup,
             "ms_per_step": tstep * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded torus of the reference's own init)", "config": cfg,
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(per), "kind": "reference",
-                             "sample": f"{len(per)} processes x ({a.warmup} warm-up + {a.steps} timed) reference "
+                             "sample": f"{len(per)} processes x ({warm} warm-up + {ktimed} timed) reference "
                                        f"steps of a {n}x{n} torus after init; wall {time.time() - t0:.0f}s"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -211,6 +222,12 @@ def b200_arm(a):
         if dist is not None:
             dist.barrier()
 
+    # advance past the start-up transient (the first steps from init run a
+    # few hundred inversions to the 200-iteration Newton limit)
+    if a.evolve:
+        h.step_ch(a.evolve)
+        h.sync()
+    t_evolved = h.sync()["t"]
     # warm-up (also instantiates the CUDA graph of one step)
     h.step_ch(a.warmup)
     h.sync()
@@ -295,10 +312,11 @@ def b200_arm(a):
                                        "RK2 midpoint, courant 0.8", "n1": n, "n2": n,
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "l2": "working set per step (geometry 126 planes x %.1f MB) exceeds L2" %
-                                 ((n + 6) * (n + 6) * 8 / 1e6)},
+                                 ((n + 6) * (n + 6) * 8 / 1e6),
+                           "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.warmup + a.steps + 1) * 2 * n * n),
+                "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:

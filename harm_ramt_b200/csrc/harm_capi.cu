@@ -42,8 +42,8 @@ struct harm_ctx {
   Grid gr;
   int n1m, n2m;
   // device buffers
-  double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin;
-  int* d_pflag;
+  double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin, *d_ubuf;
+  int *d_pflag, *d_worklist;
   unsigned char *d_bsqf, *d_chk;
   DevScalars* d_sc;
   int nblocks_flux;
@@ -78,6 +78,8 @@ struct harm_ctx {
     a.chk = d_chk;
     a.fixbuf = d_fixbuf;
     a.blockmin = d_blockmin;
+    a.ubuf = d_ubuf;
+    a.worklist = d_worklist;
     a.nblocks_flux = nblocks_flux;
     a.sc = d_sc;
     return a;
@@ -223,6 +225,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   ok &= cudaMalloc(&c->d_bsqf, (size_t)c->gr.plane) == cudaSuccess;
   ok &= cudaMalloc(&c->d_chk, 2 * (size_t)c->gr.plane) == cudaSuccess;
   ok &= cudaMalloc(&c->d_sc, sizeof(DevScalars)) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_ubuf, NPR * pd) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_worklist, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
   if (!ok) {
     harm_destroy(c);
     return HARM_ENOMEM;
@@ -267,6 +271,8 @@ void harm_destroy(harm_ctx* c)
   cudaFree(c->d_bsqf);
   cudaFree(c->d_chk);
   cudaFree(c->d_sc);
+  cudaFree(c->d_ubuf);
+  cudaFree(c->d_worklist);
   delete c;
 }
 
@@ -504,10 +510,11 @@ int harm_get_fluxes(harm_ctx* c, double* F1, double* F2)
 // that loads the library holds one copy of it until the process exits.
 static constexpr long long NOALLOC_MAX_PLANE = 5632;  // pitch * (n2 + 6): 64 x 64 interior zones fit
 static constexpr int NOALLOC_MAX_BLOCKS = 256;        // x1/x2 flux blocks of 32 x 4 zones
-static constexpr long long NA_DPLANES = 31;           // pk0 8, F1 8, F2 8, emf, gammacheck, fixbuf 5
+static constexpr long long NA_DPLANES = 39;  // pk0 8, F1 8, F2 8, emf, gammacheck, fixbuf 5, ubuf 8
 static constexpr long long NA_OFF_BLOCKMIN = NA_DPLANES * NOALLOC_MAX_PLANE;
 static constexpr long long NA_OFF_SCALARS = NA_OFF_BLOCKMIN + 2 * NOALLOC_MAX_BLOCKS;
-static constexpr long long NA_OFF_BYTES = NA_OFF_SCALARS + 32;  // 256 B for DevScalars
+static constexpr long long NA_OFF_WORKLIST = NA_OFF_SCALARS + 32;  // 256 B for DevScalars
+static constexpr long long NA_OFF_BYTES = NA_OFF_WORKLIST + NOALLOC_MAX_PLANE / 2;  // one int per zone
 static constexpr long long NA_DOUBLES = NA_OFF_BYTES + (3 * NOALLOC_MAX_PLANE) / 8 + 32;
 static_assert(sizeof(DevScalars) <= 32 * sizeof(double), "DevScalars must fit its slot");
 static __device__ __align__(256) double g_noalloc_scratch[NA_DOUBLES];
@@ -563,6 +570,8 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.d_emf = s + 24 * pl;
   c.d_gammacheck = s + 25 * pl;
   c.d_fixbuf = s + 26 * pl;
+  c.d_ubuf = s + 31 * pl;
+  c.d_worklist = (int*)(s + NA_OFF_WORKLIST);
   c.d_blockmin = s + NA_OFF_BLOCKMIN;
   c.d_sc = (DevScalars*)(s + NA_OFF_SCALARS);
   c.d_bsqf = (unsigned char*)(s + NA_OFF_BYTES);

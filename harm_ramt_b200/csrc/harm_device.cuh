@@ -315,14 +315,20 @@ __device__ __forceinline__ void func_vsq(const U2PCtx& c, double W, double vsq, 
 }
 
 // general_newton_raphson + validate_x(vartype 3), utoprim_2d.c:606-740, 556-600
-__device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x1, double gammafail, int& niter_out)
+// Returns 0/1 as the reference does, or NEWTON_DEFERRED when `maxit` (< 200)
+// iterations ran without convergence; the caller then redoes the solve with
+// the full 200 (the iteration sequence is deterministic, so the redo reaches
+// the reference's result).
+constexpr int NEWTON_DEFERRED = -7;
+__device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x1, double gammafail, int& niter_out,
+                                          int maxit)
 {
   constexpr int MAX_NEWT_ITER = 200;
   constexpr double NEWT_TOL = 1.0e-15, MIN_NEWT_TOL = 1.0e-10, W_TOO_BIG = 1.e9;
   const double vsq_too_big = (1.0 - 1.0 / (gammafail - 1.0));
   double errx = 1., errx_old = 2., errx_oldest;
   int n_iter = 0;
-  while ((errx > NEWT_TOL) && (n_iter < MAX_NEWT_ITER)) {
+  while ((errx > NEWT_TOL) && (n_iter < maxit)) {
     double dx0, dx1;
     func_vsq(c, x0, x1, dx0, dx1);
     if (((n_iter + 1) % 10) == 0) {
@@ -347,6 +353,7 @@ __device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x
     n_iter++;
   }
   niter_out = n_iter;
+  if (maxit < MAX_NEWT_ITER && n_iter >= maxit && errx > NEWT_TOL) return NEWTON_DEFERRED;
   if (n_iter >= MAX_NEWT_ITER) return (errx > MIN_NEWT_TOL) ? 1 : 0;
   return 0;
 }
@@ -368,7 +375,7 @@ __device__ __forceinline__ void lower_g(const double* v, const double* c, double
 // conserved vector (with sqrt(-g)); pr holds the guess on entry.  Returns
 // the pflag code; *niter gets the Newton iteration count.
 __device__ __forceinline__ int utoprim_2d(const double* U, const Geo<double>& g, double* pr, double gam, double gammafail,
-                                          int* niter)
+                                          int* niter, int maxit = 200)
 {
   constexpr double W_TOO_BIG = 1.e9, FAIL_VAL = 1.e30;
   double Ug[NPR], Ut[NPR], pt[NPR];
@@ -425,7 +432,8 @@ __device__ __forceinline__ int utoprim_2d(const double* U, const Geo<double>& g,
       c.wglobal = w;
       double x0 = fabs(W), ut = fabs(utsq_calc(c, W));
       double x1 = (ut > 0.) ? (ut / (ut + 1.)) : 0.0;
-      int ret = newton_vsq(c, x0, x1, gammafail, *niter);
+      int ret = newton_vsq(c, x0, x1, gammafail, *niter, maxit);
+      if (ret == NEWTON_DEFERRED) return NEWTON_DEFERRED;
       if (ret != 0) {
         pfl = ret * 100 + 1;
       } else if ((W = x0) == FAIL_VAL) {

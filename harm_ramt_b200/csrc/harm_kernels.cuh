@@ -47,6 +47,8 @@ struct DevScalars {
   int chk_changed[8];    // per-round change flags of the check-solution sweep
   int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
   int fixups;            // zones repaired by fixup_utoprim in the last step
+  int ndeferred;         // zones whose inversion went to the tail kernel (this substep)
+  int ndeferred_total;   // same, summed since the last harm_set_time
 };
 
 struct StepArgs {
@@ -62,6 +64,8 @@ struct StepArgs {
   unsigned char* chk;    // 2 planes: check-solution decisions (double buffer)
   double* fixbuf;        // 5 planes: repaired rho..u3
   double* blockmin;      // per-block dt minima: [2][nblocks]
+  double* ubuf;          // 8 planes: conserved state of zones deferred to the tail kernel
+  int* worklist;         // deferred zone indices (capacity: one plane)
   int nblocks_flux;
   DevScalars* sc;
 };

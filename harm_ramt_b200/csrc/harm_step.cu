@@ -44,35 +44,39 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
 }
 
 // ---------------------------------------------------------------- fluxes
-template <typename T, bool PARA, bool FFDE>
-__device__ __forceinline__ void face_flux(const StepArgs& a, const double* __restrict__ pb, int i, int j, int dir,
-                                          double* Fo, double& dtij)
+// Interface states of zone (i, j) along `dir` (step_ch.c:812-823 slopes and
+// 893-904 interface values): L = the zone's left-face value (p_r of face i),
+// R = its right-face value (p_l of face i+1).
+template <typename T, bool PARA>
+__device__ __forceinline__ void zone_states(const StepArgs& a, const double* __restrict__ pb, int i, int j, int dir,
+                                            T* L, T* R)
 {
-  const int di = (dir == 1), dj = (dir == 2);
-  const long long s = (long long)di + (long long)dj * a.gr.pitch;  // stride along dir
+  const long long s = (dir == 1) ? 1LL : (long long)a.gr.pitch;
   const long long z = a.gr.at(i, j);
-  T p_l[NPR], p_r[NPR];
 #pragma unroll
   for (int k = 0; k < NPR; k++) {
     const double* pk = pb + k * a.gr.plane + z;
     if (!PARA) {
-      // interface states from MC slopes of zones i-1 and i (step_ch.c:893-904)
-      T ym2 = (T)__ldg(pk - 2 * s), ym1 = (T)__ldg(pk - s), y0 = (T)__ldg(pk), yp1 = (T)__ldg(pk + s);
-      T dqm = mc_slope(ym2, ym1, y0);
-      T dq0 = mc_slope(ym1, y0, yp1);
-      p_l[k] = ym1 + T(0.5) * dqm;
-      p_r[k] = y0 - T(0.5) * dq0;
+      T ym1 = (T)__ldg(pk - s), y0 = (T)__ldg(pk), yp1 = (T)__ldg(pk + s);
+      T dq = mc_slope(ym1, y0, yp1);
+      L[k] = y0 - T(0.5) * dq;
+      R[k] = y0 + T(0.5) * dq;
     } else {
-      // right state of zone i-1 and left state of zone i from para4
-      T ym3 = (T)__ldg(pk - 3 * s), ym2 = (T)__ldg(pk - 2 * s), ym1 = (T)__ldg(pk - s), y0 = (T)__ldg(pk),
-        yp1 = (T)__ldg(pk + s), yp2 = (T)__ldg(pk + 2 * s);
       T l, r;
-      para4(ym3, ym2, ym1, y0, yp1, l, r);
-      p_l[k] = r;
-      para4(ym2, ym1, y0, yp1, yp2, l, r);
-      p_r[k] = l;
+      para4((T)__ldg(pk - 2 * s), (T)__ldg(pk - s), (T)__ldg(pk), (T)__ldg(pk + s), (T)__ldg(pk + 2 * s), l, r);
+      L[k] = l;
+      R[k] = r;
     }
   }
+}
+
+// Flux through one face from its two interface states (the rest of the
+// fluxcalc face loop, step_ch.c:944-1065).
+template <typename T, bool FFDE>
+__device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int dir, T* p_l, T* p_r, double* Fo,
+                                          double& dtij)
+{
+  const long long z = a.gr.at(i, j);
   Geo<T> g;
   load_geo(a, dir == 1 ? FACE1 : FACE2, z, g);
   // B^dir continuity (BDIRCONT, step_ch.c:944-947)
@@ -140,40 +144,67 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 
 // fluxcalc for both directions over i in [-1,N1], j in [-1,N2]: x1 faces
 // with i >= 0, x2 faces with j >= 0 (FZLOOP ranges), then the fix_flux
-// rules that do not read another face (fixup.c:1357-1410).
+// rules that do not read another face (fixup.c:1357-1410).  Blocks are
+// 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
+// states once: the x1 neighbour's right state arrives by warp shuffle and
+// the x2 neighbour's through shared memory (the first lane/row recomputes).
+constexpr int FLUX_BY = 4;
 template <typename T, bool PARA, bool FFDE>
-__global__ void __launch_bounds__(128) k_flux(StepArgs a, const double* __restrict__ pb)
+__global__ void __launch_bounds__(32 * FLUX_BY) k_flux(StepArgs a, const double* __restrict__ pb)
 {
   __shared__ double sh[2][32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
+  __shared__ T shr[NPR][FLUX_BY][32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * 32 + tx - 1;
+  const int j = blockIdx.y * FLUX_BY + ty - 1;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   const bool in = (i <= n1) && (j <= n2);
+  // threads past the grid work on a clamped (valid) zone; their results are unused
+  const int ic = (i <= n1) ? i : n1, jc = (j <= n2) ? j : n2;
   double dt1 = 1.e9, dt2 = 1.e9;
-  if (in) {
-    const long long z = a.gr.at(i, j);
-    double Fo[NPR], dtij;
-    if (i >= 0) {
-      face_flux<T, PARA, FFDE>(a, pb, i, j, 1, Fo, dtij);
-      dt1 = (dtij < dt1) ? dtij : dt1;
-      if (i == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
-      if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
+  const long long z = a.gr.at(ic, jc);
+  T L[NPR], R[NPR], pl[NPR];
+  double Fo[NPR], dtij;
+  // ---- x1 faces
+  zone_states<T, PARA>(a, pb, ic, jc, 1, L, R);
 #pragma unroll
-      for (int k = 0; k < NPR; k++) a.F1[k * a.gr.plane + z] = Fo[k];
+  for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
+  if (tx == 0 && ic >= 0) {
+    T Lm[NPR];
+    zone_states<T, PARA>(a, pb, ic - 1, jc, 1, Lm, pl);
+  }
+  if (in && i >= 0) {
+    face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij);
+    dt1 = (dtij < dt1) ? dtij : dt1;
+    if (i == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
+    if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
+#pragma unroll
+    for (int k = 0; k < NPR; k++) a.F1[k * a.gr.plane + z] = Fo[k];
+  }
+  // ---- x2 faces
+  zone_states<T, PARA>(a, pb, ic, jc, 2, L, R);
+#pragma unroll
+  for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
+  __syncthreads();
+  if (ty > 0) {
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
+  } else if (jc >= 0) {
+    T Lm[NPR];
+    zone_states<T, PARA>(a, pb, ic, jc - 1, 2, Lm, pl);
+  }
+  if (in && j >= 0) {
+    face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
+    dt2 = (dtij < dt2) ? dtij : dt2;
+    const bool polar = (j == 0 || j == n2) && (i < n1);
+    const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
+    if (polar || equator) {
+#pragma unroll
+      for (int k = 0; k < NPR; k++)
+        if (k != U2) Fo[k] = 0.;
     }
-    if (j >= 0) {
-      face_flux<T, PARA, FFDE>(a, pb, i, j, 2, Fo, dtij);
-      dt2 = (dtij < dt2) ? dtij : dt2;
-      const bool polar = (j == 0 || j == n2) && (i < n1);
-      const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
-      if (polar || equator) {
 #pragma unroll
-        for (int k = 0; k < NPR; k++)
-          if (k != U2) Fo[k] = 0.;
-      }
-#pragma unroll
-      for (int k = 0; k < NPR; k++) a.F2[k * a.gr.plane + z] = Fo[k];
-    }
+    for (int k = 0; k < NPR; k++) a.F2[k * a.gr.plane + z] = Fo[k];
   }
   dt1 = block_min(dt1, sh[0]);
   dt2 = block_min(dt2, sh[1]);
@@ -191,6 +222,7 @@ __global__ void k_emf(StepArgs a)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (i == 0 && j == 0) a.sc->ndeferred = 0;
   if (i > n1 || j > n2) return;
   const long long pl = a.gr.plane;
   const double* F1b2 = a.F1 + B2 * pl;
@@ -207,10 +239,30 @@ __global__ void k_emf(StepArgs a)
 }
 
 // ---------------------------------------------------------------- update
+// Newton iterations a zone may take inside k_update before it is handed to
+// k_update_tail (the reference's limit is 200; typical zones need 2-4).
+constexpr int NEWTON_MAIN_CAP = 16;
+
+// pflag store + fixup1zone (fixup.c:274-377: floors then the Lorentz factor
+// limit) + store of the new primitives
+__device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>& g, long long z, int i, int j, double* pfz,
+                                            int pfl, double* pf)
+{
+  const long long pl = a.gr.plane;
+  a.pflag[z] = pfl;
+  const double frho = __ldg(a.geo + (long long)GEO_FLOOR * pl + z), fu = __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z);
+  if (frho > pfz[RHO]) pfz[RHO] = frho;
+  if (fu > pfz[UU]) pfz[UU] = fu;
+  int rc = limit_gamma(a.pp.gammamax, pfz, g);
+  if (rc) report_fail(a.sc, rc, i, j);
+#pragma unroll
+  for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
+}
+
 // advance_standard zone loop, advance.c:114-181, for one RK2 substep.
 // CUf = {1, 0, c2}: Uf = Ui + c2*dt*dU; on the last substep unew = Uf.
 template <bool FFDE>
-__global__ void __launch_bounds__(128) k_update(StepArgs a, const double* __restrict__ pi, const double* __restrict__ pb,
+__global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __restrict__ pi, const double* __restrict__ pb,
                                                 double* __restrict__ pf, double c2)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -290,20 +342,46 @@ __global__ void __launch_bounds__(128) k_update(StepArgs a, const double* __rest
     }
   }
   int niter;
-  int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter);
-  a.pflag[z] = pfl;
-  // fixup1zone, fixup.c:274-377: floors then the Lorentz factor limit
-  const double frho = __ldg(a.geo + (long long)GEO_FLOOR * pl + z), fu = __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z);
-  if (frho > pfz[RHO]) pfz[RHO] = frho;
-  if (fu > pfz[UU]) pfz[UU] = fu;
-  int rc = limit_gamma(a.pp.gammamax, pfz, g);
-  if (rc) report_fail(a.sc, rc, i, j);
+  int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP);
+  if (pfl == NEWTON_DEFERRED) {
+    // rare slow inversion: hand the zone to k_update_tail so that this warp
+    // is not held for up to 200 iterations by one lane
 #pragma unroll
-  for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
+    for (int k = 0; k < NPR; k++) a.ubuf[k * pl + z] = U[k];
+    a.worklist[atomicAdd(&a.sc->ndeferred, 1)] = (int)z;
+    niter = 0;
+  } else {
+    finish_zone(a, g, z, i, j, pfz, pfl, pf);
+  }
   // Newton iteration count (the reference's nstroke), one atomic per warp
   const unsigned mask = __activemask();
   const unsigned it = __reduce_add_sync(mask, (unsigned)niter);
   if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&a.sc->newton_iters, (unsigned long long)it);
+}
+
+// The deferred inversions of k_update, redone with the full iteration limit.
+// A deferred zone's pf slot was not written, so pi still holds its guess.
+__global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __restrict__ pi, double* __restrict__ pf)
+{
+  const int nd = a.sc->ndeferred;
+  const long long pl = a.gr.plane;
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nd; w += gridDim.x * blockDim.x) {
+    const long long z = a.worklist[w];
+    const int i = (int)(z % a.gr.pitch) - NG, j = (int)(z / a.gr.pitch) - NG;
+    Geo<double> g;
+    load_geo(a, CENT, z, g);
+    double U[NPR], pfz[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) {
+      U[k] = a.ubuf[k * pl + z];
+      pfz[k] = pi[k * pl + z];
+    }
+    int niter;
+    int pfl = utoprim_2d(U, g, pfz, a.pp.gam, a.pp.gammafail, &niter);
+    finish_zone(a, g, z, i, j, pfz, pfl, pf);
+    atomicAdd(&a.sc->newton_iters, (unsigned long long)niter);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.sc->ndeferred_total += nd;
 }
 
 // ---------------------------------------------------------------- bounds
@@ -644,6 +722,7 @@ void launch_update(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const doub
                    double c2)
 {
   k_update<false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  k_update_tail<<<148, 64, 0, s>>>(a, pi, pf);
 }
 
 }  // namespace harm

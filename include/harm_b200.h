@@ -132,7 +132,7 @@ const char* harm_kernel_name(int k);
    reference.  For callers that cannot call cudaMalloc (a host code that owns
    all device memory through its own pool, or that runs where allocation is
    forbidden): the caller passes its own device buffers and the scratch of
-   the step lives in a static array compiled into this library (about 1.4 MB
+   the step lives in a static array compiled into this library (about 1.8 MB
    per device, held until the process exits).  Limit: pitch * (n2 + 6) <=
    5632 doubles per plane, i.e. at most 64 x 64 active zones; larger grids
    are rejected with HARM_EINVAL and a message on stderr.
