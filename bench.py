@@ -199,6 +199,21 @@ def reference_arm(a):
 
 
 # ------------------------------------------------------------------ b200 arm
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The job's time for a per-rank quantity: its maximum over ranks."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, zones_per_rank, seconds_per_step):
+    """Whole-job zone-cycles/s: every rank advances its own torus each step."""
+    return world * zones_per_rank / seconds_per_step
+
+
 def b200_arm(a):
     import torch
     import harm_ramt_b200 as hb
@@ -248,12 +263,9 @@ def b200_arm(a):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     st = h.sync()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     ms_step = ms / a.steps
-    value = world * n * n / (ms_step * 1e-3)
+    value = aggregate_rate(world, n * n, ms_step * 1e-3)
 
     # end to end through the C ABI with host buffers: each step uploads the
     # state from host memory, advances it and reads it back
@@ -268,12 +280,8 @@ def b200_arm(a):
         h.step_ch(1)
         host_p, host_f = h.get_prims()
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / a.e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * n * n / e2e_s
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / a.e2e_steps, dist, "cuda")
+    e2e = aggregate_rate(world, n * n, e2e_s)
 
     # roofline of the dominant kernel (largest share of the step's device time)
     peak, peak_kind = peaks()

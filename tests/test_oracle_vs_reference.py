@@ -1,0 +1,35 @@
+"""The C restatement (oracle) against the reference compiled from its own
+sources (oracle/_ref): identical initial state and geometry, bit-for-bit
+equal primitives, inversion flags, t and dt after every step.  Skipped where
+the reference build is absent (it is built from the reference tree)."""
+import numpy as np
+import pytest
+
+import harmtest as ht
+
+CASES = [(16, 3, 1, 120), (32, 4, 0, 60), (32, 4, 1, 60), (64, 3, 1, 25)]
+
+
+@pytest.mark.parametrize("n,lim,flux,nsteps", CASES)
+def test_oracle_matches_reference(n, lim, flux, nsteps):
+    r = ht.ref_run(n, n, lim=lim, flux=flux, nsteps=nsteps)
+    if r is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    o = ht.Oracle(n, n, r["geom"], lim=lim, fluxmethod=flux, **ht.ref_config(r))
+    p = r["prims"][0].copy()
+    f = r["pflag"][0].copy()
+    t, dt = r["times"][0]
+    nfixed = 0
+    for s in range(1, nsteps + 1):
+        rc, t, dt = o.step(p, f, t, dt)
+        assert rc == 0
+        assert np.array_equal(p, r["prims"][s]), f"step {s}: primitives differ"
+        assert np.array_equal(f[3:-3, 3:-3, 0], r["pflag"][s][3:-3, 3:-3, 0]), f"step {s}: flags differ"
+        assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
+        nfixed += int((f[3:-3, 3:-3, 0] == -1).sum())
+    f1, f2 = o.fluxes()
+    I = ht.interior
+    assert np.array_equal(I(f1), I(r["F1"])) and np.array_equal(I(f2), I(r["F2"]))
+    # the run exercised the Newton cycle break (the reference's count is
+    # cumulative from init, the oracle's from this run)
+    assert r["ncyclebreak"] >= o.ncyclebreak()
