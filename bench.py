@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--lim", default="para", choices=["para", "mc"])
     ap.add_argument("--flux", default="hll", choices=["hll", "laxf"])
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--evolve", type=int, default=400,
                     help="untimed steps from init before warm-up, so that the timed steps see a developed flow")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -269,16 +269,19 @@ def b200_arm(a):
 
     # end to end through the C ABI with host buffers: each step uploads the
     # state from host memory, advances it and reads it back
-    host_p, _ = h.get_prims()
-    h2d = host_p.nbytes
-    d2h = host_p.nbytes + host_p.shape[0] * host_p.shape[1] * 5 * 4
+    # (page-locked host buffers; the state of step k+1 is the output of k)
+    bufs = [(hb.pinned_empty((n + 6, n + 6, 8)), hb.pinned_empty((n + 6, n + 6, 5), np.int32)) for _ in range(2)]
+    h.get_prims(out=bufs[0])
+    h2d = bufs[0][0].nbytes
+    d2h = bufs[0][0].nbytes + bufs[0][1].nbytes
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(a.e2e_steps):
-        h.set_prims(host_p, reset_gammacheck=False)
+    for k in range(a.e2e_steps):
+        src, dst = bufs[k % 2], bufs[(k + 1) % 2]
+        h.set_prims(src[0], reset_gammacheck=False)
         h.step_ch(1)
-        host_p, host_f = h.get_prims()
+        h.get_prims(out=dst)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / a.e2e_steps, dist, "cuda")
     e2e = aggregate_rate(world, n * n, e2e_s)

@@ -211,10 +211,17 @@ class HarmGPU:
         _check(self.lib.harm_set_prims(self._h, _dp(p), None if f is None else _ip(f), int(bool(reset_gammacheck))),
                "harm_set_prims")
 
-    def get_prims(self):
-        p = np.zeros((self.n1m, self.n2m, NPR))
-        f = np.zeros((self.n1m, self.n2m, 5), dtype=np.int32)
-        _check(self.lib.harm_get_prims(self._h, _dp(p), _ip(f)), "harm_get_prims")
+    def get_prims(self, out=None, with_flags=True):
+        """Device -> host copy; `out=(prims, pflag)` reuses caller buffers
+        (pinned buffers from :func:`pinned_empty` make the copy fastest)."""
+        if out is None:
+            p = np.zeros((self.n1m, self.n2m, NPR))
+            f = np.zeros((self.n1m, self.n2m, 5), dtype=np.int32) if with_flags else None
+        else:
+            p, f = out
+            assert p.flags.c_contiguous and p.dtype == np.float64 and p.shape == (self.n1m, self.n2m, NPR)
+            assert f is None or (f.flags.c_contiguous and f.dtype == np.int32 and f.shape == (self.n1m, self.n2m, 5))
+        _check(self.lib.harm_get_prims(self._h, _dp(p), None if f is None else _ip(f)), "harm_get_prims")
         return p, f
 
     def bound_prims(self):
@@ -252,6 +259,15 @@ class HarmGPU:
         f2 = np.zeros((self.n1m, self.n2m, NPR))
         _check(self.lib.harm_get_fluxes(self._h, _dp(f1), _dp(f2)), "harm_get_fluxes")
         return f1, f2
+
+
+def pinned_empty(shape, dtype=np.float64):
+    """A page-locked host array (allocated through torch), for fast
+    host<->device copies of the reference-layout state."""
+    import torch
+    t = torch.empty(tuple(shape), dtype={np.float64: torch.float64, np.int32: torch.int32}[np.dtype(dtype).type],
+                    pin_memory=True)
+    return t.numpy()
 
 
 def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, stream=None, **torus_kw):

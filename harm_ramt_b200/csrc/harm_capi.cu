@@ -30,6 +30,8 @@ __global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
 __global__ void k_fixup_compute(StepArgs a, const double* pv);
 __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd);
 __global__ void k_dt_finalize(StepArgs a);
+__global__ void k_ref_to_planes(StepArgs a, const double* ref, const int* refflag, double* pv);
+__global__ void k_planes_to_ref(StepArgs a, const double* pv, double* ref, int* refflag);
 }  // namespace harm
 
 using namespace harm;
@@ -44,6 +46,8 @@ struct harm_ctx {
   // device buffers
   double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin, *d_ubuf;
   int *d_pflag, *d_worklist;
+  double* d_stage;   // reference-layout prims staging buffer
+  int* d_stagef;     // reference-layout pflag staging buffer
   unsigned char *d_bsqf, *d_chk;
   DevScalars* d_sc;
   int nblocks_flux;
@@ -227,6 +231,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   ok &= cudaMalloc(&c->d_sc, sizeof(DevScalars)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_ubuf, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_worklist, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_stage, (size_t)c->n1m * c->n2m * NPR * sizeof(double)) == cudaSuccess;
+  ok &= cudaMalloc(&c->d_stagef, (size_t)c->n1m * c->n2m * 5 * sizeof(int)) == cudaSuccess;
   if (!ok) {
     harm_destroy(c);
     return HARM_ENOMEM;
@@ -273,6 +279,8 @@ void harm_destroy(harm_ctx* c)
   cudaFree(c->d_sc);
   cudaFree(c->d_ubuf);
   cudaFree(c->d_worklist);
+  cudaFree(c->d_stage);
+  cudaFree(c->d_stagef);
   delete c;
 }
 
@@ -319,19 +327,16 @@ int harm_upload_geometry(harm_ctx* c, const double* gcov, const double* gcon, co
 int harm_set_prims(harm_ctx* c, const double* prims, const int* pflag, int reset_gammacheck)
 {
   if (!c || !prims) return HARM_EINVAL;
-  const int n1m = c->n1m, n2m = c->n2m;
-  const long long pl = c->gr.plane;
-  std::vector<double> h((size_t)NPR * pl, 0.0);
-  std::vector<int> hf((size_t)pl, 0);
-  for (int ii = 0; ii < n1m; ii++)
-    for (int jj = 0; jj < n2m; jj++) {
-      const long long zr = (long long)ii * n2m + jj, zd = c->gr.at(ii - NG, jj - NG);
-      for (int k = 0; k < NPR; k++) h[(size_t)k * pl + zd] = prims[zr * NPR + k];
-      if (pflag) hf[zd] = pflag[zr * 5 + 0];
-    }
-  CK(cudaMemcpyAsync(c->d_p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->d_pflag, hf.data(), hf.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  if (reset_gammacheck) CK(cudaMemsetAsync(c->d_gammacheck, 0, (size_t)pl * sizeof(double), c->stream));
+  const size_t nz = (size_t)c->n1m * c->n2m;
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  // one contiguous host->device copy, then the layout change on the device
+  CK(cudaMemcpyAsync(c->d_stage, prims, nz * NPR * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (pflag) CK(cudaMemcpyAsync(c->d_stagef, pflag, nz * 5 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  else CK(cudaMemsetAsync(c->d_pflag, 0, (size_t)c->gr.plane * sizeof(int), c->stream));
+  k_ref_to_planes<<<grid2(c->n1m, c->n2m, b), b, 0, c->stream>>>(a, c->d_stage, pflag ? c->d_stagef : nullptr, c->d_p);
+  CK(cudaGetLastError());
+  if (reset_gammacheck) CK(cudaMemsetAsync(c->d_gammacheck, 0, (size_t)c->gr.plane * sizeof(double), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return HARM_OK;
 }
@@ -339,28 +344,14 @@ int harm_set_prims(harm_ctx* c, const double* prims, const int* pflag, int reset
 int harm_get_prims(harm_ctx* c, double* prims, int* pflag)
 {
   if (!c) return HARM_EINVAL;
-  const int n1m = c->n1m, n2m = c->n2m;
-  const long long pl = c->gr.plane;
-  std::vector<double> h((size_t)NPR * pl);
-  std::vector<int> hf((size_t)pl);
-  std::vector<unsigned char> hb((size_t)pl);
-  CK(cudaMemcpyAsync(h.data(), c->d_p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(hf.data(), c->d_pflag, hf.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(hb.data(), c->d_bsqf, hb.size(), cudaMemcpyDeviceToHost, c->stream));
+  const size_t nz = (size_t)c->n1m * c->n2m;
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  k_planes_to_ref<<<grid2(c->n1m, c->n2m, b), b, 0, c->stream>>>(a, c->d_p, c->d_stage, pflag ? c->d_stagef : nullptr);
+  CK(cudaGetLastError());
+  if (prims) CK(cudaMemcpyAsync(prims, c->d_stage, nz * NPR * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (pflag) CK(cudaMemcpyAsync(pflag, c->d_stagef, nz * 5 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int ii = 0; ii < n1m; ii++)
-    for (int jj = 0; jj < n2m; jj++) {
-      const long long zr = (long long)ii * n2m + jj, zd = c->gr.at(ii - NG, jj - NG);
-      if (prims)
-        for (int k = 0; k < NPR; k++) prims[zr * NPR + k] = h[(size_t)k * pl + zd];
-      if (pflag) {
-        pflag[zr * 5 + 0] = hf[zd];
-        pflag[zr * 5 + 1] = 0;
-        pflag[zr * 5 + 2] = hb[zd] & 3;
-        pflag[zr * 5 + 3] = (hb[zd] >> 2) & 3;
-        pflag[zr * 5 + 4] = 0;
-      }
-    }
   return HARM_OK;
 }
 

@@ -711,6 +711,48 @@ __global__ void k_dt_finalize(StepArgs a)
   }
 }
 
+// ---------------------------------------------------------------- layouts
+// Reference layout (defs.h: zone (ii, jj) at ii*n2m + jj, components
+// fastest) <-> the step's planes.  Threads run along the planes' fast index
+// i, so every plane store is coalesced and every zone's 8 reference-layout
+// values are one contiguous 64 B read (or write).
+__global__ void k_ref_to_planes(StepArgs a, const double* __restrict__ ref, const int* __restrict__ refflag,
+                                double* __restrict__ pv)
+{
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n1m = a.gr.n1 + 2 * NG, n2m = a.gr.n2 + 2 * NG;
+  if (ii >= n1m || jj >= n2m) return;
+  const long long zr = (long long)ii * n2m + jj, zd = (long long)jj * a.gr.pitch + ii;
+  const double2* src = reinterpret_cast<const double2*>(ref + zr * NPR);
+#pragma unroll
+  for (int k = 0; k < NPR / 2; k++) {
+    const double2 v = __ldg(src + k);
+    pv[(2 * k) * a.gr.plane + zd] = v.x;
+    pv[(2 * k + 1) * a.gr.plane + zd] = v.y;
+  }
+  if (refflag) a.pflag[zd] = __ldg(refflag + zr * 5);
+}
+
+__global__ void k_planes_to_ref(StepArgs a, const double* __restrict__ pv, double* __restrict__ ref, int* __restrict__ refflag)
+{
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n1m = a.gr.n1 + 2 * NG, n2m = a.gr.n2 + 2 * NG;
+  if (ii >= n1m || jj >= n2m) return;
+  const long long zr = (long long)ii * n2m + jj, zd = (long long)jj * a.gr.pitch + ii;
+  double2* dst = reinterpret_cast<double2*>(ref + zr * NPR);
+#pragma unroll
+  for (int k = 0; k < NPR / 2; k++) dst[k] = make_double2(pv[(2 * k) * a.gr.plane + zd], pv[(2 * k + 1) * a.gr.plane + zd]);
+  if (refflag) {
+    const unsigned char b = a.bsqf[zd];
+    int* f = refflag + zr * 5;
+    f[0] = a.pflag[zd];
+    f[1] = 0;
+    f[2] = b & 3;
+    f[3] = (b >> 2) & 3;
+    f[4] = 0;
+  }
+}
+
 // launchers for the templated kernels (used by the host engine)
 void launch_flux(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
 {
