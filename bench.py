@@ -296,7 +296,8 @@ def b200_arm(a):
     step_alg = BYTES_PER_ZONE_CYCLE * n * n / (ms_step * 1e-3) / 1e9
     total_prof = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRAFFIC.get(dom),
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (TRAFFIC_512[dom] * (n * n) / (512 * 512)) if dom in TRAFFIC_512 else None,
                 "bytes_per_zone": KERNEL_BYTES.get(dom, 0), "launch_ms": per_launch_ms,
                 "share_of_step": dom_ms / total_prof if total_prof else None,
                 "whole_step": {"achieved": step_alg, "frac": step_alg / peak,
@@ -339,10 +340,12 @@ def b200_arm(a):
 KERNEL_BYTES = {
     "k_flux": 8 * (8 + 2 * 21 + 2 * 8),       # prims once, FACE1+FACE2 geometry, F1+F2 out
     "k_update": 8 * (8 + 8 + 21 + 40 + 2 + 2 * 8 + 1 + 8) + 4,  # pi, pb, CENT geo, conn, floors, 2 faces x2, emf, pf, pflag
-    "k_emf": 8 * (2 + 5 + 1),
+    "k_emf": 8 * (2 + 3 + 1),
     "k_bsqflags": 8 * (8 + 21) + 1,
 }
-TRAFFIC = {}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
+# at 512^2 (profiles/k_*_torus512_fp64_para_hll.md), scaled by zone count
+TRAFFIC_512 = {"k_flux": 109.3e6, "k_update": 194.1e6}
 
 
 def main():
