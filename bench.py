@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--evolve", type=int, default=400,
                     help="untimed steps from init before warm-up, so that the timed steps see a developed flow")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--accuracy-t", type=float, default=100.0,
+                    help="time (GM/c^3) to which FP64 and mixed runs go from init for the L1 comparison")
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
@@ -304,6 +307,9 @@ def b200_arm(a):
                                "bytes_per_zone_cycle": BYTES_PER_ZONE_CYCLE},
                 "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()}}
 
+    mixed = None
+    if not a.no_mixed:
+        mixed = mixed_precision_leg(a, hb, stream, lim, flux, value, barrier, dist)
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -327,13 +333,71 @@ def b200_arm(a):
                                  ((n + 6) * (n + 6) * 8 / 1e6),
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def _run_to(h, tf):
+    while True:
+        h.step_ch(500)
+        st = h.sync()
+        if st["t"] >= tf:
+            return st
+
+
+def mixed_precision_leg(a, hb, stream, lim, flux, value_fp64, barrier, dist):
+    """The mixed form: throughput on the same developed torus, and relative
+    L1 errors against FP64 for runs from init to t = accuracy_t."""
+    import torch
+    n = a.n
+    hm, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=hb.PREC_MIXED, stream=stream.cuda_stream)
+    if a.evolve:
+        hm.step_ch(a.evolve)
+    hm.step_ch(a.warmup)
+    hm.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    hm.step_ch(a.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda") / a.steps
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    vm = aggregate_rate(world, n * n, ms * 1e-3)
+    prof = hm.profile_step()
+    hm.close()
+    out = {"value": vm, "unit": UNIT, "ms_per_step": ms, "speedup_vs_fp64": vm / value_fp64,
+           "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()}}
+    if a.accuracy_t > 0:
+        res = {}
+        for prec in (hb.PREC_FP64, hb.PREC_MIXED):
+            h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=prec, tf=a.accuracy_t,
+                                       stream=stream.cuda_stream)
+            try:
+                st = _run_to(h, a.accuracy_t)
+            except hb.HarmError as e:
+                st = h.sync(raise_on_fail=False)
+                out["l1_vs_fp64"] = {"t": a.accuracy_t, "error": f"{'fp64' if prec == hb.PREC_FP64 else 'mixed'} "
+                                                                  f"run stopped at t={st['t']:.4g}: {e}"}
+                h.close()
+                return out
+            p, _ = h.get_prims(with_flags=False)
+            res[prec] = (p[3:-3, 3:-3], h.get_horizon(), st)
+            h.close()
+        pd, hd, sd = res[hb.PREC_FP64]
+        pm, hm_, sm = res[hb.PREC_MIXED]
+        l1 = lambda x, y: float(np.abs(x - y).sum() / np.abs(y).sum())
+        out["l1_vs_fp64"] = {"t": a.accuracy_t, "rho": l1(pm[..., 0], pd[..., 0]), "u": l1(pm[..., 1], pd[..., 1]),
+                             "B": l1(pm[..., 5:8], pd[..., 5:8]),
+                             "horizon_mass_flux_integrated": abs(hm_["pcum_rho"] - hd["pcum_rho"]) / abs(hd["pcum_rho"]),
+                             "steps_fp64": sd["realnstep"], "steps_mixed": sm["realnstep"]}
+    return out
 
 
 # algorithmic bytes per active zone of one launch (FP64, see DESIGN.md)

@@ -23,13 +23,15 @@ import os
 import numpy as np
 
 __all__ = ["HarmGPU", "HarmError", "torus_params", "torus_geometry", "torus_init", "load_library", "LIB_PATH",
-           "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "NG", "NPR"]
+           "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "PREC_FP64", "PREC_MIXED", "NG", "NPR", "pinned_empty",
+           "torus_context"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libharm_b200.so")
 NG = 3
 NPR = 8
 LIM_MC, LIM_PARA = 3, 4
 FLUX_LAXF, FLUX_HLL = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
 
 _ERRORS = {0: "ok", 1: "invalid argument", 2: "no usable CUDA device (sm_100 required)", 3: "CUDA runtime error",
            4: "device allocation failed", 5: "geometry tables missing or not symmetric",
@@ -47,7 +49,7 @@ class HarmError(RuntimeError):
 
 class _Config(ctypes.Structure):
     _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("lim", ctypes.c_int), ("fluxmethod", ctypes.c_int),
-                ("eom", ctypes.c_int), ("reserved", ctypes.c_int), ("cour", ctypes.c_double),
+                ("eom", ctypes.c_int), ("precision", ctypes.c_int), ("cour", ctypes.c_double),
                 ("gam", ctypes.c_double), ("dx1", ctypes.c_double), ("dx2", ctypes.c_double),
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
                 ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
@@ -74,7 +76,7 @@ _lib = None
 EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
            "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
-           "harm_kernel_name"]
+           "harm_kernel_name", "harm_get_horizon"]
 
 
 def load_library(path=None):
@@ -112,6 +114,7 @@ def load_library(path=None):
     lib.harm_torus_geometry.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp, dp, dp]
     lib.harm_torus_init.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
     lib.harm_profile_step.argtypes = [vp, dp, ip, ctypes.c_int]
+    lib.harm_get_horizon.argtypes = [vp, dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
     if path is None:
@@ -176,11 +179,11 @@ class HarmGPU:
 
     def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
-                 stream=None):
+                 precision=PREC_FP64, stream=None):
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
-        cfg = _Config(n1, n2, lim, fluxmethod, 0, 0, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+        cfg = _Config(n1, n2, lim, fluxmethod, 0, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
                       bsqorholimit, bsqoulimit, tf)
         h = ctypes.c_void_p()
         _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
@@ -248,11 +251,19 @@ class HarmGPU:
 
     def profile_step(self):
         """One step with a CUDA event after every kernel: {name: (ms, launches)}."""
-        nk = 12
+        nk = 13
         ms = np.zeros(nk)
         n = np.zeros(nk, dtype=np.int32)
         _check(self.lib.harm_profile_step(self._h, _dp(ms), _ip(n), nk), "harm_profile_step")
         return {self.lib.harm_kernel_name(k).decode(): (float(ms[k]), int(n[k])) for k in range(nk)}
+
+    def get_horizon(self):
+        """diag_flux()'s inner-face accounting: dict of pdot_rho, pdot_uu,
+        em_bsq_term (pdotterms[3][UU]), em_bb_term (pdotterms[6][UU]),
+        pcum_rho, pcum_uu."""
+        out = np.zeros(6)
+        _check(self.lib.harm_get_horizon(self._h, _dp(out)), "harm_get_horizon")
+        return dict(zip(("pdot_rho", "pdot_uu", "em_bsq_term", "em_bb_term", "pcum_rho", "pcum_uu"), out.tolist()))
 
     def get_fluxes(self):
         f1 = np.zeros((self.n1m, self.n2m, NPR))
@@ -270,7 +281,8 @@ def pinned_empty(shape, dtype=np.float64):
     return t.numpy()
 
 
-def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, stream=None, **torus_kw):
+def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, precision=PREC_FP64, tf=1.0e30,
+                  stream=None, **torus_kw):
     """Builds the benchmark torus on the host and returns (HarmGPU, geometry,
     initial prims) with the state uploaded, bounded and t=0, dt=1e-5 set as
     init_defglobal() leaves them (initbase.c:158)."""
@@ -278,7 +290,7 @@ def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, 
     geom = torus_geometry(par)
     p0 = torus_init(par, geom)
     h = HarmGPU(n1, n2, geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, cour=cour, gam=par.gam,
-                gammamax=par.gammamax, stream=stream)
+                gammamax=par.gammamax, precision=precision, tf=tf, stream=stream)
     h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
     h.set_prims(p0)
     h.bound_prims()

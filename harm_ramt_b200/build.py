@@ -11,14 +11,17 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libharm_b200.so")
-SOURCES = ["harm_capi.cu", "harm_step.cu", "setup_torus.cpp"]
-HEADERS = ["harm_device.cuh", "harm_kernels.cuh", "../../include/harm_b200.h", "../../include/harm_setup.h"]
+SOURCES = ["harm_capi.cu", "harm_step.cu", "harm_step_mixed.cu", "setup_torus.cpp"]
+HEADERS = ["harm_device.cuh", "harm_kernels.cuh", "harm_step_impl.cuh", "../../include/harm_b200.h",
+           "../../include/harm_setup.h"]
 
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
-]
+COMMON = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
+# FP64 path: no contraction, IEEE division/square root (bit parity with the reference)
+EXACT = ["--fmad=false"]
+# mixed-precision instantiations only: contraction and fast FP32 division/sqrt
+FAST = ["--fmad=true", "--prec-div=false", "--prec-sqrt=false", "--ftz=true"]
+FLAGS = {"harm_step_mixed.cu": FAST}
+NVCC_FLAGS = COMMON + EXACT  # kept for reference by tools that print the build line
 
 
 def _nvcc():
@@ -39,12 +42,24 @@ def needs_build():
 def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+    import tempfile
+    objs = []
+    with tempfile.TemporaryDirectory(prefix="harm_build_") as tmp:
+        for src in SOURCES:
+            obj = os.path.join(tmp, src + ".o")
+            cmd = [_nvcc()] + COMMON + FLAGS.get(src, EXACT) + ["-c", os.path.join(CSRC, src), "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+            objs.append(obj)
+        cmd = [_nvcc()] + COMMON + ["-shared", "-o", LIB + ".tmp"] + objs
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

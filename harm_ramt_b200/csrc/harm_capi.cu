@@ -18,10 +18,11 @@
 
 namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
-void launch_flux(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
-__global__ void k_emf(StepArgs a);
-void launch_update(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb, double* pf,
-                   double c2);
+void launch_flux(int para, int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_update(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
+                   double* pf, double c2);
+void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
 __global__ void k_gammacheck(StepArgs a, const double* pv);
@@ -45,6 +46,7 @@ struct harm_ctx {
   int n1m, n2m;
   // device buffers
   double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin, *d_ubuf;
+  float* d_geo32;
   int *d_pflag, *d_worklist;
   double* d_stage;   // reference-layout prims staging buffer
   int* d_stagef;     // reference-layout pflag staging buffer
@@ -73,6 +75,7 @@ struct harm_ctx {
     a.pp.bsqoulimit = cfg.bsqoulimit;
     a.pp.tf = cfg.tf;
     a.geo = d_geo;
+    a.geo32 = d_geo32;
     a.F1 = d_F1;
     a.F2 = d_F2;
     a.emf = d_emf;
@@ -103,10 +106,10 @@ static dim3 grid2(int ni, int nj, dim3 b) { return dim3((ni + b.x - 1) / b.x, (n
 
 // kernel classes of one step, in launch order (for per-kernel timing)
 enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_CHECKSOL, KC_CHECKSERIAL, KC_FIXC,
-       KC_FIXA, KC_DT, KC_COUNT };
+       KC_FIXA, KC_DT, KC_HORIZON, KC_COUNT };
 static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", "k_update", "k_bound", "k_poledeath",
                                                "k_gammacheck", "k_checksol", "k_checksol_serial", "k_fixup_compute",
-                                               "k_fixup_apply", "k_dt_finalize"};
+                                               "k_fixup_apply", "k_dt_finalize", "k_horizon"};
 
 struct Timer {
   // records an event after every launch when active
@@ -138,11 +141,12 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
     const double c2 = (sub == 0) ? 0.5 : 1.0;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
+    const int mixed = c->cfg.precision == HARM_PREC_MIXED;
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
     T.mark(s, KC_FLUX);
-    k_emf<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a);
+    launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
-    launch_update(grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
+    launch_update(mixed, grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE);
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
@@ -165,6 +169,8 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
     T.mark(s, KC_POLE);
   }
+  launch_horizon(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
+  T.mark(s, KC_HORIZON);
   k_dt_finalize<<<1, 1024, 0, s>>>(a);
   T.mark(s, KC_DT);
   return cudaGetLastError() == cudaSuccess ? HARM_OK : HARM_ECUDA;
@@ -190,7 +196,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
 {
   if (!cfg || !out) return HARM_EINVAL;
   *out = nullptr;
-  if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->reserved != 0) return HARM_EINVAL;
+  if (cfg->n1 < 4 || cfg->n2 < 4) return HARM_EINVAL;
+  if (cfg->precision != HARM_PREC_FP64 && cfg->precision != HARM_PREC_MIXED) return HARM_EINVAL;
   if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
   if (cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
@@ -219,6 +226,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   ok &= cudaMalloc(&c->d_p, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_pk0, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_geo, GEO_NPLANES * pd) == cudaSuccess;
+  if (cfg->precision == HARM_PREC_MIXED)
+    ok &= cudaMalloc(&c->d_geo32, 2 * GEO_PER_LOC * (size_t)c->gr.plane * sizeof(float)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_F1, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_F2, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_emf, pd) == cudaSuccess;
@@ -267,6 +276,7 @@ void harm_destroy(harm_ctx* c)
   cudaFree(c->d_p);
   cudaFree(c->d_pk0);
   cudaFree(c->d_geo);
+  cudaFree(c->d_geo32);
   cudaFree(c->d_F1);
   cudaFree(c->d_F2);
   cudaFree(c->d_emf);
@@ -319,6 +329,13 @@ int harm_upload_geometry(harm_ctx* c, const double* gcov, const double* gcon, co
       h[(size_t)(GEO_FLOOR + 1) * pl + zd] = floors[zr * 2 + 1];
     }
   CK(cudaMemcpyAsync(c->d_geo, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  std::vector<float> h32;
+  if (c->d_geo32) {
+    // FP32 copies of the two face locations (FACE1, FACE2 are the first 42 planes)
+    h32.resize((size_t)2 * GEO_PER_LOC * pl);
+    for (size_t k = 0; k < h32.size(); k++) h32[k] = (float)h[k];
+    CK(cudaMemcpyAsync(c->d_geo32, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->geo_ok = true;
   return HARM_OK;
@@ -454,14 +471,35 @@ int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)
 
 const char* harm_kernel_name(int k) { return (k >= 0 && k < KC_COUNT) ? KC_NAMES[k] : ""; }
 
+int harm_get_horizon(harm_ctx* c, double* out)
+{
+  if (!c || !out) return HARM_EINVAL;
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 6; k++) out[k] = h.hz[k];
+  return HARM_OK;
+}
+
 int harm_get_fluxes(harm_ctx* c, double* F1, double* F2)
 {
   if (!c || !F1 || !F2) return HARM_EINVAL;
   const int n1 = c->cfg.n1, n2 = c->cfg.n2, n1m = c->n1m, n2m = c->n2m;
   const long long pl = c->gr.plane;
   std::vector<double> h1((size_t)NPR * pl), h2((size_t)NPR * pl), he((size_t)pl);
-  CK(cudaMemcpyAsync(h1.data(), c->d_F1, h1.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(h2.data(), c->d_F2, h2.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (c->cfg.precision == HARM_PREC_MIXED) {
+    std::vector<float> f1((size_t)NPR * pl), f2((size_t)NPR * pl);
+    CK(cudaMemcpyAsync(f1.data(), c->d_F1, f1.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(f2.data(), c->d_F2, f2.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < h1.size(); k++) {
+      h1[k] = f1[k];
+      h2[k] = f2[k];
+    }
+  } else {
+    CK(cudaMemcpyAsync(h1.data(), c->d_F1, h1.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(h2.data(), c->d_F2, h2.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaMemcpyAsync(he.data(), c->d_emf, he.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   auto D = [&](int i, int j) { return c->gr.at(i, j); };
@@ -516,7 +554,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
                                  double* dt, int reset_gammacheck, void* stream)
 {
   if (!cfg || !d_geo || !d_prims || !d_pflag || !t || !dt) return HARM_EINVAL;
-  if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->reserved != 0 || cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
+  if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->precision != HARM_PREC_FP64 || cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
   if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
   harm_ctx c;

@@ -148,7 +148,9 @@ __device__ __forceinline__ void flux_of(const T* pr, const State<T>& q, int dir,
 template <typename T>
 __device__ __forceinline__ int vchar_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T& vmax, T& vmin)
 {
-  const T eps100 = T(DBL_EPS_REF * 100.0);
+  // NUMEPSILON*100 of the reference's FTYPE (global.h:706-727): DBL_EPSILON
+  // for FP64, FLT_EPSILON for the FP32 faces of the mixed form
+  const T eps100 = (sizeof(T) == 8) ? T(DBL_EPS_REF * 100.0) : T(1.19209290e-07 * 100.0);
   T bsq = dot4(q.bcon, q.bcov);
   T rho = pr[RHO], u = pr[UU];
   T WW = rho + gam * u, cs2, EF, va2;
@@ -185,8 +187,12 @@ __device__ __forceinline__ int vchar_of(const T* pr, const State<T>& q, int dir,
   T B = T(2.) * (AuBu - (AB + AuBu) * cms2);
   T C = Au2 - (Asq + Au2) * cms2;
   T discr = B * B - T(4.) * A * C;
-  if ((discr < T(0.0)) && (discr > T(-1E-10))) discr = T(0.0);
-  else if (discr < T(-1E-10)) return FAIL_VCHAR_DISCR;
+  // the reference's absolute -1e-10 round-off allowance (vchar.c:203); FP32
+  // faces (mixed form) allow round-off relative to the terms, 100 FLT_EPSILON
+  const T dtol = (sizeof(T) == 8) ? T(1E-10)
+                                  : fmax(T(1E-10), T(1.19209290e-07 * 100.0) * (B * B + fabs(T(4.) * A * C)));
+  if ((discr < T(0.0)) && (discr > -dtol)) discr = T(0.0);
+  else if (discr < -dtol) return FAIL_VCHAR_DISCR;
   discr = sqrt(discr);
   T vm = -(-B + discr) / (T(2.) * A);
   T vp = -(-B - discr) / (T(2.) * A);

@@ -46,7 +46,8 @@ struct DevScalars {
   unsigned long long newton_iters;   // Newton iterations since the last reset
   int chk_changed[8];    // per-round change flags of the check-solution sweep
   int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
-  int fixups;            // zones repaired by fixup_utoprim in the last step
+  int fixups;            // zones repaired by fixup_utoprim since the last harm_set_time
+  double hz[6];          // horizon accounting of the last step (see k_horizon)
   int ndeferred;         // zones whose inversion went to the tail kernel (this substep)
   int ndeferred_total;   // same, summed since the last harm_set_time
 };
@@ -55,8 +56,9 @@ struct StepArgs {
   Grid gr;
   Params pp;
   const double* geo;     // GEO_NPLANES planes
-  double* F1;            // 8 planes
-  double* F2;            // 8 planes
+  const float* geo32;    // mixed precision: FACE1 and FACE2 geometry (2 x 21 float planes)
+  double* F1;            // 8 planes (of float in mixed precision)
+  double* F2;            // 8 planes (of float in mixed precision)
   double* emf;           // 1 plane
   int* pflag;            // 1 plane (FLAGUTOPRIMFAIL)
   unsigned char* bsqf;   // 1 plane: (b^2/rho flag) | (b^2/u flag) << 2
@@ -73,6 +75,17 @@ struct StepArgs {
 __device__ __forceinline__ void report_fail(DevScalars* sc, int code, int i, int j)
 {
   if (atomicCAS(&sc->status, 0, code) == 0) sc->status_zone = (i + NG) + 100000 * (j + NG);
+}
+
+// FP32 copy of a face location's geometry (mixed precision)
+__device__ __forceinline__ void load_geo32(const StepArgs& a, int loc, long long z, Geo<float>& g)
+{
+  const float* base = a.geo32 + (long long)loc * GEO_PER_LOC * a.gr.plane + z;
+#pragma unroll
+  for (int c = 0; c < 10; c++) g.gcov[c] = __ldg(base + c * a.gr.plane);
+#pragma unroll
+  for (int c = 0; c < 10; c++) g.gcon[c] = __ldg(base + (10 + c) * a.gr.plane);
+  g.g = __ldg(base + 20 * a.gr.plane);
 }
 
 template <typename T>

@@ -13,7 +13,7 @@
 //   k_fixup_*      fixup_utoprim from a snapshot
 //   k_bound/k_poledeath again, and k_dt_finalize after the last substep.
 #include <cuda_runtime.h>
-#include "harm_kernels.cuh"
+#include "harm_step_impl.cuh"
 
 namespace harm {
 
@@ -41,322 +41,6 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
   else if (bsq / pr[UU] > 0.9 * a.pp.bsqoulimit) f3 = 1;
   else f3 = 0;
   a.bsqf[z] = (unsigned char)(f0 | (f3 << 2));
-}
-
-// ---------------------------------------------------------------- fluxes
-// Interface states of zone (i, j) along `dir` (step_ch.c:812-823 slopes and
-// 893-904 interface values): L = the zone's left-face value (p_r of face i),
-// R = its right-face value (p_l of face i+1).
-template <typename T, bool PARA>
-__device__ __forceinline__ void zone_states(const StepArgs& a, const double* __restrict__ pb, int i, int j, int dir,
-                                            T* L, T* R)
-{
-  const long long s = (dir == 1) ? 1LL : (long long)a.gr.pitch;
-  const long long z = a.gr.at(i, j);
-#pragma unroll
-  for (int k = 0; k < NPR; k++) {
-    const double* pk = pb + k * a.gr.plane + z;
-    if (!PARA) {
-      T ym1 = (T)__ldg(pk - s), y0 = (T)__ldg(pk), yp1 = (T)__ldg(pk + s);
-      T dq = mc_slope(ym1, y0, yp1);
-      L[k] = y0 - T(0.5) * dq;
-      R[k] = y0 + T(0.5) * dq;
-    } else {
-      T l, r;
-      para4((T)__ldg(pk - 2 * s), (T)__ldg(pk - s), (T)__ldg(pk), (T)__ldg(pk + s), (T)__ldg(pk + 2 * s), l, r);
-      L[k] = l;
-      R[k] = r;
-    }
-  }
-}
-
-// Flux through one face from its two interface states (the rest of the
-// fluxcalc face loop, step_ch.c:944-1065).
-template <typename T, bool FFDE>
-__device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int dir, T* p_l, T* p_r, double* Fo,
-                                          double& dtij)
-{
-  const long long z = a.gr.at(i, j);
-  Geo<T> g;
-  load_geo(a, dir == 1 ? FACE1 : FACE2, z, g);
-  // B^dir continuity (BDIRCONT, step_ch.c:944-947)
-  const int bd = B1 + dir - 1;
-  p_l[bd] = p_r[bd] = T(0.5) * (p_l[bd] + p_r[bd]);
-  const T gmax = (T)a.pp.gammamax, gam = (T)a.pp.gam;
-  int rc = limit_gamma(gmax, p_l, g);
-  if (!rc) rc = limit_gamma(gmax, p_r, g);
-  State<T> ql, qr;
-  state_of(p_l, g, ql);
-  state_of(p_r, g, qr);
-  T F_l[NPR], F_r[NPR], U_l[NPR], U_r[NPR];
-  flux_of<T, FFDE>(p_l, ql, dir, g, gam, F_l);
-  flux_of<T, FFDE>(p_r, qr, dir, g, gam, F_r);
-  flux_of<T, FFDE>(p_l, ql, 0, g, gam, U_l);
-  flux_of<T, FFDE>(p_r, qr, 0, g, gam, U_r);
-  T cmax_l, cmin_l, cmax_r, cmin_r;
-  if (!rc) rc = vchar_of(p_l, ql, dir, g, gam, cmax_l, cmin_l);
-  if (!rc) rc = vchar_of(p_r, qr, dir, g, gam, cmax_r, cmin_r);
-  if (rc) {
-    report_fail(a.sc, rc, i, j);
-    cmax_l = cmin_l = cmax_r = cmin_r = T(0.);
-  }
-  // cminmax_calc, step_ch.c:1095-1148
-  T lmin = rmin(cmin_l, cmin_r), lmax = rmax(cmax_l, cmax_r);
-  lmin = fabs(rmax(T(0.), -lmin));
-  lmax = fabs(rmax(T(0.), lmax));
-  T cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
-  const T hllfrac = (a.pp.fluxmethod == 1) ? T(1.0) : T(0.0);
-  const T laxffrac = (a.pp.fluxmethod == 1) ? T(0.0) : T(1.0);
-  if (cmax + cmin != T(0.0)) {
-#pragma unroll
-    for (int k = 0; k < NPR; k++)
-      Fo[k] = (double)(hllfrac * ((cmax * F_l[k] + cmin * F_r[k] - cmax * cmin * (U_r[k] - U_l[k])) / (cmax + cmin)) +
-                       laxffrac * (T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k]))));
-  } else {
-#pragma unroll
-    for (int k = 0; k < NPR; k++) Fo[k] = (double)(T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k])));
-  }
-  // face Courant limit, step_ch.c:1062-1065 (kept in FP64)
-  double cm = (double)rmax(cmax, cmin);
-  dtij = a.pp.cour * (dir == 1 ? a.pp.dx1 : a.pp.dx2) / cm;
-}
-
-__device__ __forceinline__ double block_min(double v, double* sh)
-{
-  // exact minimum (no rounding), NaN-ignoring like `if (x < m) m = x`
-  for (int o = 16; o > 0; o >>= 1) {
-    double w = __shfl_down_sync(0xffffffffu, v, o);
-    v = (w < v) ? w : v;
-  }
-  const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31, warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
-  if (lane == 0) sh[warp] = v;
-  __syncthreads();
-  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
-  if (warp == 0) {
-    v = (lane < nw) ? sh[lane] : 1.e9;
-    for (int o = 16; o > 0; o >>= 1) {
-      double w = __shfl_down_sync(0xffffffffu, v, o);
-      v = (w < v) ? w : v;
-    }
-  }
-  return v;
-}
-
-// fluxcalc for both directions over i in [-1,N1], j in [-1,N2]: x1 faces
-// with i >= 0, x2 faces with j >= 0 (FZLOOP ranges), then the fix_flux
-// rules that do not read another face (fixup.c:1357-1410).  Blocks are
-// 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
-// states once: the x1 neighbour's right state arrives by warp shuffle and
-// the x2 neighbour's through shared memory (the first lane/row recomputes).
-constexpr int FLUX_BY = 4;
-template <typename T, bool PARA, bool FFDE>
-__global__ void __launch_bounds__(32 * FLUX_BY) k_flux(StepArgs a, const double* __restrict__ pb)
-{
-  __shared__ double sh[2][32];
-  __shared__ T shr[NPR][FLUX_BY][32];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i = blockIdx.x * 32 + tx - 1;
-  const int j = blockIdx.y * FLUX_BY + ty - 1;
-  const int n1 = a.gr.n1, n2 = a.gr.n2;
-  const bool in = (i <= n1) && (j <= n2);
-  // threads past the grid work on a clamped (valid) zone; their results are unused
-  const int ic = (i <= n1) ? i : n1, jc = (j <= n2) ? j : n2;
-  double dt1 = 1.e9, dt2 = 1.e9;
-  const long long z = a.gr.at(ic, jc);
-  T L[NPR], R[NPR], pl[NPR];
-  double Fo[NPR], dtij;
-  // ---- x1 faces
-  zone_states<T, PARA>(a, pb, ic, jc, 1, L, R);
-#pragma unroll
-  for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
-  if (tx == 0 && ic >= 0) {
-    T Lm[NPR];
-    zone_states<T, PARA>(a, pb, ic - 1, jc, 1, Lm, pl);
-  }
-  if (in && i >= 0) {
-    face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij);
-    dt1 = (dtij < dt1) ? dtij : dt1;
-    if (i == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
-    if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
-#pragma unroll
-    for (int k = 0; k < NPR; k++) a.F1[k * a.gr.plane + z] = Fo[k];
-  }
-  // ---- x2 faces
-  zone_states<T, PARA>(a, pb, ic, jc, 2, L, R);
-#pragma unroll
-  for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
-  __syncthreads();
-  if (ty > 0) {
-#pragma unroll
-    for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
-  } else if (jc >= 0) {
-    T Lm[NPR];
-    zone_states<T, PARA>(a, pb, ic, jc - 1, 2, Lm, pl);
-  }
-  if (in && j >= 0) {
-    face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
-    dt2 = (dtij < dt2) ? dtij : dt2;
-    const bool polar = (j == 0 || j == n2) && (i < n1);
-    const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
-    if (polar || equator) {
-#pragma unroll
-      for (int k = 0; k < NPR; k++)
-        if (k != U2) Fo[k] = 0.;
-    }
-#pragma unroll
-    for (int k = 0; k < NPR; k++) a.F2[k * a.gr.plane + z] = Fo[k];
-  }
-  dt1 = block_min(dt1, sh[0]);
-  dt2 = block_min(dt2, sh[1]);
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    const int b = blockIdx.y * gridDim.x + blockIdx.x;
-    a.blockmin[b] = dt1;
-    a.blockmin[a.nblocks_flux + b] = dt2;
-  }
-}
-
-// flux_ct corner EMF, step_ch.c:1214-1234, over i in [0,N1], j in [0,N2].
-// F1 on the rows j = -1 and j = N2 carries fix_flux's mirrored B2 for i < N1.
-__global__ void k_emf(StepArgs a)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int n1 = a.gr.n1, n2 = a.gr.n2;
-  if (i == 0 && j == 0) a.sc->ndeferred = 0;
-  if (i > n1 || j > n2) return;
-  const long long pl = a.gr.plane;
-  const double* F1b2 = a.F1 + B2 * pl;
-  const double* F2b1 = a.F2 + B1 * pl;
-  double f1a = F1b2[a.gr.at(i, j)];
-  if (j == n2 && i < n1) f1a = -F1b2[a.gr.at(i, n2 - 1)];
-  double f1b = F1b2[a.gr.at(i, j - 1)];
-  if (j - 1 == -1 && i < n1) f1b = -F1b2[a.gr.at(i, 0)];
-  double f2a = F2b1[a.gr.at(i, j)], f2b = F2b1[a.gr.at(i - 1, j)];
-  const double gc = gdet_at(a, CORN, a.gr.at(i, j));
-  const double g1 = gdet_at(a, FACE1, a.gr.at(i, j)), g2 = gdet_at(a, FACE1, a.gr.at(i, j - 1));
-  const double g3 = gdet_at(a, FACE2, a.gr.at(i, j)), g4 = gdet_at(a, FACE2, a.gr.at(i - 1, j));
-  a.emf[a.gr.at(i, j)] = 0.25 * (gc) * (f1a / (g1) + f1b / (g2) - f2a / (g3) - f2b / (g4));
-}
-
-// ---------------------------------------------------------------- update
-// Newton iterations a zone may take inside k_update before it is handed to
-// k_update_tail (the reference's limit is 200; typical zones need 2-4).
-constexpr int NEWTON_MAIN_CAP = 16;
-
-// pflag store + fixup1zone (fixup.c:274-377: floors then the Lorentz factor
-// limit) + store of the new primitives
-__device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>& g, long long z, int i, int j, double* pfz,
-                                            int pfl, double* pf)
-{
-  const long long pl = a.gr.plane;
-  a.pflag[z] = pfl;
-  const double frho = __ldg(a.geo + (long long)GEO_FLOOR * pl + z), fu = __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z);
-  if (frho > pfz[RHO]) pfz[RHO] = frho;
-  if (fu > pfz[UU]) pfz[UU] = fu;
-  int rc = limit_gamma(a.pp.gammamax, pfz, g);
-  if (rc) report_fail(a.sc, rc, i, j);
-#pragma unroll
-  for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
-}
-
-// advance_standard zone loop, advance.c:114-181, for one RK2 substep.
-// CUf = {1, 0, c2}: Uf = Ui + c2*dt*dU; on the last substep unew = Uf.
-template <bool FFDE>
-__global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __restrict__ pi, const double* __restrict__ pb,
-                                                double* __restrict__ pf, double c2)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= a.gr.n1 || j >= a.gr.n2) return;
-  const long long pl = a.gr.plane, z = a.gr.at(i, j);
-  const double dt = a.sc->dt;
-  Geo<double> g;
-  load_geo(a, CENT, z, g);
-  const double gam = a.pp.gam;
-  double U[NPR], pfz[NPR];
-  {
-    // Ui = U(pi)
-    double pr[NPR];
-#pragma unroll
-    for (int k = 0; k < NPR; k++) pr[k] = __ldg(pi + k * pl + z);
-#pragma unroll
-    for (int k = 0; k < NPR; k++) pfz[k] = pr[k];
-    State<double> q;
-    state_of(pr, g, q);
-    flux_of<double, FFDE>(pr, q, 0, g, gam, U);
-  }
-  double dUg[NPR];
-  {
-    // source_conn, phys.c:520-619: dU[UU+l] = e * sum_j sum_k T^j_k Gamma^k_{lj}
-    double pr[NPR];
-#pragma unroll
-    for (int k = 0; k < NPR; k++) pr[k] = __ldg(pb + k * pl + z);
-    State<double> q;
-    state_of(pr, g, q);
-    double acc[4] = {0., 0., 0., 0.};
-    const double* cn = a.geo + z;
-#pragma unroll
-    for (int jj = 0; jj < 4; jj++) {
-      double row[4];
-      mhd_row<double, FFDE>(pr, jj, q, gam, row);
-#pragma unroll
-      for (int l = 0; l < 4; l++)
-#pragma unroll
-        for (int k = 0; k < 4; k++) acc[l] += row[k] * __ldg(cn + (long long)conn_plane(k, l, jj) * pl);
-    }
-    dUg[RHO] = 0. + g.g * 0.;
-    dUg[B1] = dUg[B2] = dUg[B3] = dUg[RHO];
-#pragma unroll
-    for (int l = 0; l < 4; l++) dUg[UU + l] = 0. + g.g * acc[l];
-  }
-  {
-    // flux divergence with flux-CT B fluxes (step_ch.c:1403-1413) and the
-    // RK combine of dUtoU, advance.c:273-286
-    const double idx1 = 1.0 / a.pp.dx1, idx2 = 1.0 / a.pp.dx2;
-    const long long zi1 = a.gr.at(i + 1, j), zj1 = a.gr.at(i, j + 1), zij = a.gr.at(i + 1, j + 1);
-    const double e00 = a.emf[z], e10 = a.emf[zi1], e01 = a.emf[zj1], e11 = a.emf[zij];
-    const double cdt = c2 * dt;
-#pragma unroll
-    for (int k = 0; k < NPR; k++) {
-      double f1p, f1m, f2p, f2m;
-      if (k == B1) {
-        f1p = 0.;
-        f1m = 0.;
-        f2m = -0.5 * (e00 + e10);
-        f2p = -0.5 * (e01 + e11);
-      } else if (k == B2) {
-        f1m = 0.5 * (e00 + e01);
-        f1p = 0.5 * (e10 + e11);
-        f2p = 0.;
-        f2m = 0.;
-      } else {
-        f1p = a.F1[k * pl + zi1];
-        f1m = a.F1[k * pl + z];
-        f2p = a.F2[k * pl + zj1];
-        f2m = a.F2[k * pl + z];
-      }
-      const double dU1 = (-(f1p - f1m) * idx1);
-      const double dU2 = (-(f2p - f2m) * idx2);
-      const double dUr = dU1 + dU2;
-      U[k] = 1.0 * U[k] + 0.0 * 0.0 + cdt * (dUr + dUg[k]);
-    }
-  }
-  int niter;
-  int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP);
-  if (pfl == NEWTON_DEFERRED) {
-    // rare slow inversion: hand the zone to k_update_tail so that this warp
-    // is not held for up to 200 iterations by one lane
-#pragma unroll
-    for (int k = 0; k < NPR; k++) a.ubuf[k * pl + z] = U[k];
-    a.worklist[atomicAdd(&a.sc->ndeferred, 1)] = (int)z;
-    niter = 0;
-  } else {
-    finish_zone(a, g, z, i, j, pfz, pfl, pf);
-  }
-  // Newton iteration count (the reference's nstroke), one atomic per warp
-  const unsigned mask = __activemask();
-  const unsigned it = __reduce_add_sync(mask, (unsigned)niter);
-  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&a.sc->newton_iters, (unsigned long long)it);
 }
 
 // The deferred inversions of k_update, redone with the full iteration limit.
@@ -753,18 +437,38 @@ __global__ void k_planes_to_ref(StepArgs a, const double* __restrict__ pv, doubl
   }
 }
 
-// launchers for the templated kernels (used by the host engine)
-void launch_flux(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+// launchers for the FP64 instantiations (the mixed ones live in harm_step_mixed.cu)
+void launch_flux_mixed(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_update_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
+                         double* pf, double c2);
+void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv);
+
+void launch_flux(int para, int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
 {
-  if (para) k_flux<double, true, false><<<g, b, 0, s>>>(a, pb);
+  if (mixed) launch_flux_mixed(para, g, b, s, a, pb);
+  else if (para) k_flux<double, true, false><<<g, b, 0, s>>>(a, pb);
   else k_flux<double, false, false><<<g, b, 0, s>>>(a, pb);
 }
 
-void launch_update(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb, double* pf,
-                   double c2)
+void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a)
 {
-  k_update<false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  if (mixed) launch_emf_mixed(g, b, s, a);
+  else k_emf<double><<<g, b, 0, s>>>(a);
+}
+
+void launch_update(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
+                   double* pf, double c2)
+{
+  if (mixed) launch_update_mixed(g, b, s, a, pi, pb, pf, c2);
+  else k_update<double, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
   k_update_tail<<<148, 64, 0, s>>>(a, pi, pf);
+}
+
+void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)
+{
+  if (mixed) launch_horizon_mixed(s, a, pv);
+  else k_horizon<double><<<1, 1024, 0, s>>>(a, pv);
 }
 
 }  // namespace harm

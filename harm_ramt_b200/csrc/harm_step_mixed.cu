@@ -1,0 +1,27 @@
+// Mixed-precision instantiations of the step kernels: FP32 interface states,
+// wavespeeds and face fluxes (FP32 face geometry, FP32 flux storage), with
+// the con-to-prim solve, conserved update, geometric source, EMF and dt in
+// FP64.  This translation unit is built with multiply-add contraction and
+// fast FP32 division and square root; it is not bit-identical to the
+// reference (harm_step.cu is).
+#include "harm_step_impl.cuh"
+
+namespace harm {
+
+void launch_flux_mixed(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+{
+  if (para) k_flux<float, true, false><<<g, b, 0, s>>>(a, pb);
+  else k_flux<float, false, false><<<g, b, 0, s>>>(a, pb);
+}
+
+void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a) { k_emf<float><<<g, b, 0, s>>>(a); }
+
+void launch_update_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
+                         double* pf, double c2)
+{
+  k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+}
+
+void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv) { k_horizon<float><<<1, 1024, 0, s>>>(a, pv); }
+
+}  // namespace harm

@@ -53,6 +53,12 @@ extern "C" {
 #define HARM_FLUX_HLL 1
 #define HARM_EOM_GRMHD 0
 
+/* arithmetic of the step */
+#define HARM_PREC_FP64 0   /* everything FP64: bit-identical to the reference */
+#define HARM_PREC_MIXED 1  /* reconstruction, wavespeeds and face fluxes in FP32 (FP32 face
+                              geometry and flux storage); con-to-prim, conserved update,
+                              geometric source, EMF and dt in FP64 */
+
 /* Run-time knobs of the reference (initbase.c:119-243 and the problem's
    init_global), plus the grid size that the reference fixes at compile time
    (global.h:126-127). */
@@ -61,7 +67,7 @@ typedef struct harm_config {
   int lim;              /* HARM_LIM_MC or HARM_LIM_PARA */
   int fluxmethod;       /* HARM_FLUX_HLL or HARM_FLUX_LAXF */
   int eom;              /* HARM_EOM_GRMHD */
-  int reserved;         /* must be 0 */
+  int precision;        /* HARM_PREC_FP64 or HARM_PREC_MIXED */
   double cour;          /* Courant factor */
   double gam;           /* adiabatic index */
   double dx1, dx2;      /* uniform coordinate spacings dx[1], dx[2] */
@@ -77,7 +83,7 @@ typedef struct harm_config {
 typedef struct harm_status {
   int fail_code;                 /* reference fail() code, 0 if none */
   int fail_i, fail_j;            /* zone of the first fatal check */
-  int fixups;                    /* zones repaired by fixup_utoprim, last step */
+  int fixups;                    /* zones repaired by fixup_utoprim since harm_set_time */
   long long realnstep;
   double t, dt;                  /* time and the next step's dt */
   unsigned long long newton_iters; /* Newton iterations since harm_set_time */
@@ -121,10 +127,19 @@ int harm_sync(harm_ctx* ctx, harm_status* st);
    the reference layout [n1m][n2m][8] (what diag_flux() reads). */
 int harm_get_fluxes(harm_ctx* ctx, double* F1, double* F2);
 
+/* Horizon accounting of the reference's diag_flux() (diag.c:576-833) for
+   the inner x1 face of the whole grid, computed on the device every step:
+   out[0..5] = pdot[X1DN][RHO], pdot[X1DN][UU] (face fluxes of the last step
+   in diagnostic form, summed over x2), pdotterms[X1DN][3][UU] and
+   pdotterms[X1DN][6][UU] (the b^2 u^r u_t and -b^r b_t parts of the energy
+   flux from the zone-centred state), pcum[X1DN][RHO], pcum[X1DN][UU]
+   (sum of pdot * dt since harm_set_time). */
+int harm_get_horizon(harm_ctx* ctx, double* out);
+
 /* Diagnostics: runs one step outside the graph with a CUDA event after
    every kernel and returns, per kernel class (harm_kernel_name(k), k <
    HARM_NKERNELS), the summed device time in ms and the launch count. */
-#define HARM_NKERNELS 12
+#define HARM_NKERNELS 13
 int harm_profile_step(harm_ctx* ctx, double* ms, int* launches, int nclasses);
 const char* harm_kernel_name(int k);
 
@@ -149,7 +164,7 @@ const char* harm_kernel_name(int k);
    make it before any stream capture.  Every call shares the one array:
    calls that overlap on the GPU race.  The fixup_checksolution gamma table
    (static in the reference, fixup.c:393) carries over between calls unless
-   reset_gammacheck != 0. */
+   reset_gammacheck != 0.  Only cfg->precision == HARM_PREC_FP64. */
 int harm_step_noalloc(const harm_config* cfg, const double* d_geo, double* d_prims, int* d_pflag, double* t,
                       double* dt, int reset_gammacheck, void* stream);
 

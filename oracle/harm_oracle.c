@@ -69,6 +69,7 @@ struct ho_state {
   const double *gcov, *gcon, *gdet, *conn, *floors;
   double *pk0, *dq, *pl, *pr, *F1, *F2, *emf, *prc, *ulast, *unew;
   double *gammacheck; /* persistent, [n1+2][n2+2] like fixup.c:393 */
+  double hz[6];       /* horizon accounting, see ho_get_horizon */
   long ncb;
   int fail;
 };
@@ -966,6 +967,43 @@ int ho_utoprim(ho_state *s, int i, int j, const double *U, double *pr)
   return utoprimgen(s, U, &g, pr, &s->ncb);
 }
 
+/* diag_flux() for the global region's inner x1 face, diag.c:576-833: the
+   fluxes in diagnostic form summed over j, the stress terms 3 and 6 of the
+   energy equation from the zone-centred state, and pcum += pdot * Dt */
+static void horizon_flux(ho_state *s, const double *p, double Dt)
+{
+  const int n2 = s->c.n2;
+  const double surface = s->c.dx2 * (2.0 * M_PI);
+  double pr = 0, pu = 0, t3 = 0, t6 = 0;
+  int j;
+  for (j = 0; j < n2; j++) {
+    geo gf = getgeo(s, 0, j, FACE1);
+    const double *F = P(s->F1, 0, j);
+    double Fr = F[RHO] * surface, Fu = F[UU] * surface;
+    double gr = Fr / gf.g, gu = Fu / gf.g;
+    gu += -gr;
+    pr += gr * gf.g;
+    pu += gu * gf.g;
+    geo gc = getgeo(s, 0, j, CENT);
+    ostate q;
+    state_of(P(p, 0, j), &gc, &q);
+    double bsq = 0;
+    int l;
+    for (l = 0; l < 4; l++) bsq += (q.bcon[l]) * (q.bcov[l]);
+    double surgdet = (gc.g) * surface;
+    t3 += bsq * (q.ucon[1]) * (q.ucov[0]) * surgdet;
+    t6 += -(q.bcon[1]) * (q.bcov[0]) * surgdet;
+  }
+  s->hz[0] = pr;
+  s->hz[1] = pu;
+  s->hz[2] = t3;
+  s->hz[3] = t6;
+  s->hz[4] += pr * Dt;
+  s->hz[5] += pu * Dt;
+}
+
+void ho_get_horizon(const ho_state *s, double *out) { memcpy(out, s->hz, sizeof(s->hz)); }
+
 /* step_ch_simplempi with the midpoint RK2 of setup_rktimestep,
    step_ch.c:35-188 and 412-429 */
 int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
@@ -987,6 +1025,7 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
       if ((rc = fixup_utoprim(s, pf, pflag))) return rc;
     if ((rc = bound_prims(s, pf))) return rc;
   }
+  horizon_flux(s, p, *dt);
   *t += *dt;
   if (ndt > s->c.safe * *dt) ndt = s->c.safe * *dt;
   *dt = ndt;

@@ -49,6 +49,11 @@ void ho_bsqflags(ho_state *s, const double *prims, int *pflag);
 /* last substep's fluxes F1, F2 [n1m][n2m][8] (after flux-CT) */
 void ho_get_fluxes(const ho_state *s, double *f1, double *f2);
 
+/* horizon accounting of diag_flux() (diag.c:576-833) after the last step:
+   pdot[X1DN][RHO], pdot[X1DN][UU], pdotterms[X1DN][3][UU] and [6][UU],
+   pcum[X1DN][RHO], pcum[X1DN][UU] (cumulative since creation) */
+void ho_get_horizon(const ho_state *s, double *out);
+
 /* count of Newton cycle-break events since creation */
 long ho_ncyclebreak(const ho_state *s);
 

@@ -201,6 +201,19 @@ void hr_get_floors(double *out)
   }
 }
 
+/* horizon accounting of diag_flux() (diag.c:576-833), global region, inner
+   x1 face: pdot[X1DN][RHO], pdot[X1DN][UU], pdotterms[X1DN][3][UU],
+   pdotterms[X1DN][6][UU] of the last step, pcum[X1DN][RHO], pcum[X1DN][UU] */
+void hr_get_horizon(double *out)
+{
+  out[0] = pdotreg[GLOBALENERREGION][X1DN][RHO];
+  out[1] = pdotreg[GLOBALENERREGION][X1DN][UU];
+  out[2] = pdottermsreg[GLOBALENERREGION][X1DN][3][UU];
+  out[3] = pdottermsreg[GLOBALENERREGION][X1DN][6][UU];
+  out[4] = pcumreg[GLOBALENERREGION][X1DN][RHO];
+  out[5] = pcumreg[GLOBALENERREGION][X1DN][UU];
+}
+
 /* one step of the run loop (main.c:35-45 without diagnostics/postdt) */
 int hr_step(int nsteps)
 {

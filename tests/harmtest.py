@@ -57,6 +57,7 @@ def oracle_lib():
         lib.ho_bound.argtypes = [vp, dp]
         lib.ho_bsqflags.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
         lib.ho_get_fluxes.argtypes = [vp, dp, dp]
+        lib.ho_get_horizon.argtypes = [vp, dp]
         lib.ho_ncyclebreak.argtypes = [vp]
         lib.ho_ncyclebreak.restype = ctypes.c_long
         lib.ho_cycle_break_uniform.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int]
@@ -110,6 +111,11 @@ class Oracle:
     def ncyclebreak(self):
         return self.lib.ho_ncyclebreak(self.h)
 
+    def horizon(self):
+        out = np.zeros(6)
+        self.lib.ho_get_horizon(self.h, _dp(out))
+        return out
+
 
 # ---------------------------------------------------------------- reference
 def ref_lib_path(n1, n2, problem="torus"):
@@ -144,7 +150,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     lib.hr_get_geometry(V(geom["gcov"]), V(geom["gcon"]), V(geom["gdet"]), V(geom["conn"]))
     lib.hr_get_floors(V(geom["floors"]))
     scal0 = s.copy()
-    ps, pfs, ts = [], [], []
+    ps, pfs, ts, hz = [], [], [], []
     for n in range(nsteps + 1):
         p = np.zeros((m1, m2, 8))
         pf = np.zeros((m1, m2, 5), dtype=np.int32)
@@ -154,6 +160,9 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
         ps.append(p)
         pfs.append(pf)
         ts.append((s[0], s[1]))
+        h6 = np.zeros(6)
+        lib.hr_get_horizon(V(h6))
+        hz.append(h6)
         if n < nsteps:
             os.dup2(devnull, 2)
             rcs = lib.hr_step(1)
@@ -164,7 +173,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     f2 = np.zeros((m1, m2, 8))
     lib.hr_get_fluxes(V(f1), V(f2))
     with open(outpath, "wb") as f:
-        pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, F1=f1, F2=f2,
+        pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, horizon=hz, F1=f1, F2=f2,
                          ncyclebreak=lib.hr_get_ncyclebreak()), f, protocol=4)
 
 

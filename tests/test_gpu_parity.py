@@ -56,6 +56,7 @@ def test_gpu_matches_oracle_torus32(harm, lim, flux, nsteps):
         pg, fg = h.get_prims()
         _assert_same(pg, fg, po, fo, f"step {s + 1}")
         assert st["t"] == t and st["dt"] == dt, (st, t, dt)
+        assert list(h.get_horizon().values()) == list(o.horizon()), f"step {s + 1}: horizon accounting"
     f1g, f2g = h.get_fluxes()
     f1o, f2o = o.fluxes()
     assert np.array_equal(f1g[3:-3, 3:-3], f1o[3:-3, 3:-3]) and np.array_equal(f2g[3:-3, 3:-3], f2o[3:-3, 3:-3])
@@ -73,6 +74,7 @@ def test_gpu_matches_reference_torus32(harm):
         pg, fg = h.get_prims()
         _assert_same(I(pg), fg, I(r["prims"][s]), r["pflag"][s], f"step {s}")
         assert (st["t"], st["dt"]) == tuple(r["times"][s])
+        assert list(h.get_horizon().values()) == list(r["horizon"][s]), f"step {s}: horizon accounting"
 
 
 @pytest.mark.slow

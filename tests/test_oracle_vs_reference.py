@@ -26,6 +26,7 @@ def test_oracle_matches_reference(n, lim, flux, nsteps):
         assert np.array_equal(p, r["prims"][s]), f"step {s}: primitives differ"
         assert np.array_equal(f[3:-3, 3:-3, 0], r["pflag"][s][3:-3, 3:-3, 0]), f"step {s}: flags differ"
         assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
+        assert np.array_equal(o.horizon(), r["horizon"][s]), f"step {s}: horizon accounting differs"
         nfixed += int((f[3:-3, 3:-3, 0] == -1).sum())
     f1, f2 = o.fluxes()
     I = ht.interior
