@@ -76,7 +76,7 @@ _lib = None
 EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
            "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
-           "harm_kernel_name", "harm_get_horizon"]
+           "harm_kernel_name", "harm_get_horizon", "harm_set_end_time"]
 
 
 def load_library(path=None):
@@ -102,6 +102,7 @@ def load_library(path=None):
     lib.harm_get_prims.argtypes = [vp, dp, ip]
     lib.harm_bound_prims.argtypes = [vp]
     lib.harm_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]
+    lib.harm_set_end_time.argtypes = [vp, ctypes.c_double]
     lib.harm_step.argtypes = [vp, ctypes.c_int]
     lib.harm_sync.argtypes = [vp, ctypes.POINTER(_Status)]
     lib.harm_get_fluxes.argtypes = [vp, dp, dp]
@@ -183,6 +184,7 @@ class HarmGPU:
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
+        self.safe = safe
         cfg = _Config(n1, n2, lim, fluxmethod, 0, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
                       bsqorholimit, bsqoulimit, tf)
         h = ctypes.c_void_p()
@@ -232,6 +234,29 @@ class HarmGPU:
 
     def set_time(self, t, dt, realnstep=0):
         _check(self.lib.harm_set_time(self._h, t, dt, realnstep), "harm_set_time")
+
+    def set_end_time(self, tf):
+        """Moves the end time (dt is clamped so that t + dt <= tf)."""
+        _check(self.lib.harm_set_end_time(self._h, float(tf)), "harm_set_end_time")
+
+    def run_to(self, tf, max_chunk=500):
+        """Advances until t reaches tf and returns the status.  The end time
+        is moved to tf, so the last step is clamped onto it, and steps are
+        enqueued in chunks that cannot pass tf even if dt grows by the
+        factor ``safe`` every step (a step past the end time runs at dt = 0
+        and would still re-invert every zone)."""
+        import math
+        self.set_end_time(tf)
+        st = self.sync()
+        g = self.safe
+        while st["t"] < tf:
+            if st["dt"] <= 0.0:
+                raise HarmError(1, f"run_to: dt = {st['dt']} at t = {st['t']} < {tf}")
+            x = (tf - st["t"]) / st["dt"]
+            k = int(math.log1p((g - 1.0) * x) / math.log(g)) if g > 1.0 else int(x)
+            self.step_ch(min(max(k, 1), max_chunk))
+            st = self.sync()
+        return st
 
     def step_ch(self, nsteps=1):
         """Enqueue nsteps reference steps (asynchronous)."""

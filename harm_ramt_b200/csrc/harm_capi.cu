@@ -392,9 +392,29 @@ int harm_set_time(harm_ctx* c, double t, double dt, long long realnstep)
   memset(&h, 0, sizeof(h));
   h.t = t;
   h.dt = dt;
+  h.dt_free = dt;
   h.realnstep = realnstep;
   CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return HARM_OK;
+}
+
+int harm_set_end_time(harm_ctx* c, double tf)
+{
+  if (!c || !(tf == tf)) return HARM_EINVAL;
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // the clamp of step_ch.c:183 redone for the new end time on the unclamped dt
+  h.dt = (h.t + h.dt_free > tf) ? tf - h.t : h.dt_free;
+  CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->cfg.tf = tf;
+  if (c->have_graph) {  // the end time is a launch parameter of the captured step
+    cudaGraphExecDestroy(c->gexec);
+    cudaGraphDestroy(c->graph);
+    c->have_graph = false;
+  }
   return HARM_OK;
 }
 

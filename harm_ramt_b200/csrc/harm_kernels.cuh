@@ -40,6 +40,7 @@ struct Params {
 // device-resident scalars of the run (one struct in device memory)
 struct DevScalars {
   double t, dt, ndt;
+  double dt_free;        // the next dt before the end-time clamp
   long long realnstep;
   int status;            // first fatal fail code (0 = ok)
   int status_zone;       // i + (n1+6)*j of the first failure (+ offsets)

@@ -387,10 +387,12 @@ __global__ void k_dt_finalize(StepArgs a)
     DevScalars* s = a.sc;
     double ndt = a.pp.defcon * 1. / (1. / m1 + 1. / m2);
     s->ndt = ndt;
+    const bool moved = s->dt > 0.;
     s->t += s->dt;
     s->realnstep += 1;
     if (ndt > a.pp.safe * s->dt) ndt = a.pp.safe * s->dt;
     s->dt = ndt;
+    if (moved) s->dt_free = ndt;  // a step at dt = 0 (past the end time) keeps the last one
     if (s->t + s->dt > a.pp.tf) s->dt = a.pp.tf - s->t;
   }
 }

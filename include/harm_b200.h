@@ -115,6 +115,12 @@ int harm_bound_prims(harm_ctx* ctx);
 /* Sets t, dt and realnstep (as init() or a restart leaves them). */
 int harm_set_time(harm_ctx* ctx, double t, double dt, long long realnstep);
 
+/* Changes the end time tf of the run, e.g. to stop at a diagnostic time
+   and continue.  The clamp t + dt <= tf (step_ch.c:183) is redone on the
+   unclamped next dt, so a run that stopped at the old end time moves on;
+   the state and the horizon accumulators are kept. */
+int harm_set_end_time(harm_ctx* ctx, double tf);
+
 /* Enqueues nsteps full steps of step_ch() on the context's stream
    (asynchronous; the first call captures a CUDA graph of one step). */
 int harm_step(harm_ctx* ctx, int nsteps);

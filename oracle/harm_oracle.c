@@ -70,6 +70,7 @@ struct ho_state {
   double *pk0, *dq, *pl, *pr, *F1, *F2, *emf, *prc, *ulast, *unew;
   double *gammacheck; /* persistent, [n1+2][n2+2] like fixup.c:393 */
   double hz[6];       /* horizon accounting, see ho_get_horizon */
+  double dt_free;     /* the last step's next dt before the end-time clamp */
   long ncb;
   int fail;
 };
@@ -941,6 +942,13 @@ ho_state *ho_create(const ho_config *cfg, const double *gcov, const double *gcon
   return s;
 }
 
+void ho_set_end_time(ho_state *s, double tf, double t, double *dt)
+{
+  double base = (s->dt_free > 0.) ? s->dt_free : *dt;
+  s->c.tf = tf;
+  *dt = (t + base > tf) ? tf - t : base;
+}
+
 void ho_destroy(ho_state *s)
 {
   if (!s) return;
@@ -1011,7 +1019,7 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
   static const double CUf[2][3] = {{1.0, 0.0, 0.5}, {1.0, 0.0, 1.0}};
   static const double Cunew[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 1.0}};
   double ndt = 0.0;
-  int to, rc;
+  int to, rc, moved;
   for (to = 0; to < 2; to++) {
     const double *pi = p;
     const double *pb = (to == 0) ? p : s->pk0;
@@ -1026,9 +1034,11 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
     if ((rc = bound_prims(s, pf))) return rc;
   }
   horizon_flux(s, p, *dt);
+  moved = *dt > 0.;
   *t += *dt;
   if (ndt > s->c.safe * *dt) ndt = s->c.safe * *dt;
   *dt = ndt;
+  if (moved) s->dt_free = ndt; /* a step at dt = 0 (past the end time) keeps the last one */
   if (*t + *dt > s->c.tf) *dt = s->c.tf - *t;
   return 0;
 }

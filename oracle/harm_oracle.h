@@ -41,6 +41,10 @@ void ho_destroy(ho_state *s);
    nonzero FAIL_* code of the reference when a fatal check fired. */
 int ho_step(ho_state *s, double *prims, int *pflag, double *t, double *dt);
 
+/* moves the end time tf of the run and redoes the clamp t + dt <= tf
+   (step_ch.c:183) on the last step's unclamped dt (on *dt before any step) */
+void ho_set_end_time(ho_state *s, double tf, double t, double *dt);
+
 /* Boundary fill of a prims array (bounds.fishmon.c:14) and pre_fixup flags
    (fixup.c:1197), as init() leaves them. */
 void ho_bound(ho_state *s, double *prims);

@@ -55,6 +55,8 @@ def oracle_lib():
         lib.ho_destroy.argtypes = [vp]
         lib.ho_step.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), dp, dp]
         lib.ho_bound.argtypes = [vp, dp]
+        lib.ho_set_end_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+        lib.ho_set_end_time.restype = None
         lib.ho_bsqflags.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
         lib.ho_get_fluxes.argtypes = [vp, dp, dp]
         lib.ho_get_horizon.argtypes = [vp, dp]
@@ -89,6 +91,12 @@ class Oracle:
         if getattr(self, "h", None):
             self.lib.ho_destroy(self.h)
             self.h = None
+
+    def set_end_time(self, tf, t, dt):
+        """moves the end time; returns the re-clamped dt"""
+        d = ctypes.c_double(dt)
+        self.lib.ho_set_end_time(self.h, tf, t, ctypes.byref(d))
+        return d.value
 
     def bound(self, p):
         p = np.ascontiguousarray(p, dtype=np.float64).copy()

@@ -12,11 +12,7 @@ TOL = {"rho": 1e-4, "u": 1e-4, "B": 1e-3, "mdot": 1e-4}
 
 def _run(harm, n, precision, tf):
     h, geom, p0 = harm.torus_context(n, n, lim=harm.LIM_PARA, fluxmethod=harm.FLUX_HLL, precision=precision, tf=tf)
-    while True:
-        h.step_ch(200)
-        st = h.sync()
-        if st["t"] >= tf:
-            break
+    st = h.run_to(tf)
     p, f = h.get_prims()
     hz = h.get_horizon()
     h.close()

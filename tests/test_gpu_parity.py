@@ -62,6 +62,31 @@ def test_gpu_matches_oracle_torus32(harm, lim, flux, nsteps):
     assert np.array_equal(f1g[3:-3, 3:-3], f1o[3:-3, 3:-3]) and np.array_equal(f2g[3:-3, 3:-3], f2o[3:-3, 3:-3])
 
 
+def test_end_time_clamp_matches_oracle(harm):
+    """The run stops exactly on a moved end time and continues from it as
+    the oracle does (the last step clamped onto each end time)."""
+    n = 32
+    par = harm.torus_params(n, n)
+    geom = harm.torus_geometry(par)
+    p0 = harm.torus_init(par, geom)
+    o = ht.Oracle(n, n, geom, lim=4, fluxmethod=1, dx1=geom["dx1"], dx2=geom["dx2"])
+    po = o.bound(p0)
+    fo = np.zeros(po.shape[:2] + (5,), dtype=np.int32)
+    h = _gpu_from(harm, n, geom, p0, None, 0.0, 1e-5, 4, 1)
+    h.bound_prims()
+    t, dt, nstep = 0.0, 1e-5, 0
+    for tf in (0.05, 0.2):
+        dt = o.set_end_time(tf, t, dt)
+        while t < tf:
+            rc, t, dt = o.step(po, fo, t, dt)
+            assert rc == 0
+            nstep += 1
+        st = h.run_to(tf)
+        assert st["t"] == t == tf and st["dt"] == dt == 0.0 and st["realnstep"] == nstep
+        pg, fg = h.get_prims()
+        _assert_same(pg, fg, po, fo, f"at t={tf}")
+
+
 def test_gpu_matches_reference_torus32(harm):
     r = ht.ref_run(32, 32, lim=3, flux=1, nsteps=25)
     if r is None:
