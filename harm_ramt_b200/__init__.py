@@ -23,8 +23,8 @@ import os
 import numpy as np
 
 __all__ = ["HarmGPU", "HarmError", "torus_params", "torus_geometry", "torus_init", "load_library", "LIB_PATH",
-           "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "PREC_FP64", "PREC_MIXED", "NG", "NPR", "pinned_empty",
-           "torus_context"]
+           "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "PREC_FP64", "PREC_MIXED", "EOM_GRMHD", "EOM_FFDE",
+           "BC_TORUS", "BC_STAR", "NG", "NPR", "pinned_empty", "torus_context"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libharm_b200.so")
 NG = 3
@@ -32,13 +32,16 @@ NPR = 8
 LIM_MC, LIM_PARA = 3, 4
 FLUX_LAXF, FLUX_HLL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+EOM_GRMHD, EOM_FFDE = 0, 1
+BC_TORUS, BC_STAR = 0, 1
 
 _ERRORS = {0: "ok", 1: "invalid argument", 2: "no usable CUDA device (sm_100 required)", 3: "CUDA runtime error",
            4: "device allocation failed", 5: "geometry tables missing or not symmetric",
            6: "fatal check of the reference step fired"}
 # fail() codes of the reference, global.h:562-579
 FAIL_NAMES = {1: "UTOPRIM_NEG", 2: "UTOPRIM_TEST", 3: "VCHAR_DISCR", 4: "COEFF_NEG", 5: "COEFF_SUP",
-              6: "UTCALC_DISCR", 7: "FAIL_LDZ", 8: "FAIL_BCFIX", 9: "FAIL_VSQ_NEG"}
+              6: "UTCALC_DISCR", 7: "FAIL_LDZ", 8: "FAIL_BCFIX", 9: "FAIL_VSQ_NEG",
+              20: "FFDE_SPACELIKE (Utoprim_ffde, phys.ffde.c:281)"}
 
 
 class HarmError(RuntimeError):
@@ -53,7 +56,8 @@ class _Config(ctypes.Structure):
                 ("gam", ctypes.c_double), ("dx1", ctypes.c_double), ("dx2", ctypes.c_double),
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
                 ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
-                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double)]
+                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
+                ("omegastar", ctypes.c_double)]
 
 
 class _Status(ctypes.Structure):
@@ -180,13 +184,13 @@ class HarmGPU:
 
     def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
-                 precision=PREC_FP64, stream=None):
+                 precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0):
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
         self.safe = safe
-        cfg = _Config(n1, n2, lim, fluxmethod, 0, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                      bsqorholimit, bsqoulimit, tf)
+        cfg = _Config(n1, n2, lim, fluxmethod, eom, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+                      bsqorholimit, bsqoulimit, tf, bc, omegastar)
         h = ctypes.c_void_p()
         _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
         self._h = h

@@ -18,11 +18,6 @@
 
 namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
-void launch_flux(int para, int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
-void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
-void launch_update(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
-                   double* pf, double c2);
-void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
 __global__ void k_gammacheck(StepArgs a, const double* pv);
@@ -63,6 +58,9 @@ struct harm_ctx {
     a.gr = gr;
     a.pp.lim = cfg.lim;
     a.pp.fluxmethod = cfg.fluxmethod;
+    a.pp.eom = cfg.eom;
+    a.pp.bc = cfg.bc;
+    a.pp.omegastar = cfg.omegastar;
     a.pp.cour = cfg.cour;
     a.pp.gam = cfg.gam;
     a.pp.dx1 = cfg.dx1;
@@ -87,6 +85,7 @@ struct harm_ctx {
     a.blockmin = d_blockmin;
     a.ubuf = d_ubuf;
     a.worklist = d_worklist;
+    a.pstep = d_p;
     a.nblocks_flux = nblocks_flux;
     a.sc = d_sc;
     return a;
@@ -142,16 +141,23 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
     const double c2 = (sub == 0) ? 0.5 : 1.0;
     const int mixed = c->cfg.precision == HARM_PREC_MIXED;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
+    const int ffde = c->cfg.eom == HARM_EOM_FFDE;
+    const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
     T.mark(s, KC_FLUX);
     launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
-    launch_update(mixed, grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
+    launch_update(mixed, ffde, grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE);
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
-    k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
-    T.mark(s, KC_POLE);
+    if (poledeath) {
+      k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
+      T.mark(s, KC_POLE);
+    }
+    // force-free: no b^2 flags (so no check-solution votes) and no
+    // fixup_utoprim (fixup.c:542); the second bound would repeat the first
+    if (ffde) continue;
     k_gammacheck<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pf);
     T.mark(s, KC_GCHECK);
     for (int r = 0; r < CHK_ROUNDS; r++) {
@@ -162,12 +168,14 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     T.mark(s, KC_CHECKSERIAL);
     k_fixup_compute<<<grid2(n1, n2, b), b, 0, s>>>(a, pf);
     T.mark(s, KC_FIXC);
-    k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, c->cfg.eom == HARM_EOM_GRMHD);
+    k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_FIXA);
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 0);
     T.mark(s, KC_BOUND);
-    k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
-    T.mark(s, KC_POLE);
+    if (poledeath) {
+      k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
+      T.mark(s, KC_POLE);
+    }
   }
   launch_horizon(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
   T.mark(s, KC_HORIZON);
@@ -200,7 +208,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   if (cfg->precision != HARM_PREC_FP64 && cfg->precision != HARM_PREC_MIXED) return HARM_EINVAL;
   if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
-  if (cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
+  if (cfg->eom != HARM_EOM_GRMHD && cfg->eom != HARM_EOM_FFDE) return HARM_EINVAL;
+  if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
   int dev = 0, ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HARM_ENODEVICE;
   CK(cudaGetDevice(&dev));
@@ -577,6 +586,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   if (cfg->n1 < 4 || cfg->n2 < 4 || cfg->precision != HARM_PREC_FP64 || cfg->eom != HARM_EOM_GRMHD) return HARM_EINVAL;
   if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
+  if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
   harm_ctx c;
   memset(&c, 0, sizeof(c));
   c.cfg = *cfg;
@@ -632,6 +642,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   memset(&h, 0, sizeof(h));
   h.t = *t;
   h.dt = *dt;
+  h.dt_free = *dt;
   CK(cudaMemcpyAsync(c.d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c.stream));
   if (reset_gammacheck) CK(cudaMemsetAsync(c.d_gammacheck, 0, (size_t)pl * sizeof(double), c.stream));
   int rc = enqueue_step(&c);

@@ -21,6 +21,9 @@ enum { PF_FIXED = -1, PF_NOFAIL = 0, PF_CONVUTSQ = 2, PF_CONVW = 3, PF_CONVUTSQ2
        PF_UNEG = 6, PF_RHOUNEG = 7, PF_GAMMAPERC = 8, PF_UPERC = 9 };
 // fatal fail codes, global.h:562-579
 enum { FAIL_VCHAR_DISCR = 3, FAIL_COEFF_NEG = 4, FAIL_COEFF_SUP = 5, FAIL_UTCALC_DISCR = 6, FAIL_VSQ_NEG = 9 };
+// Utoprim_ffde's space-like drift velocity (phys.ffde.c:281-284): the
+// reference aborts the step through MYFUN without a FAIL_* number
+constexpr int FAIL_FFDE_SPACELIKE = 20;
 
 constexpr double DBL_EPS_REF = 2.2204460492503131e-16;  // global.h:710
 
@@ -361,6 +364,73 @@ __device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x
   niter_out = n_iter;
   if (maxit < MAX_NEWT_ITER && n_iter >= maxit && errx > NEWT_TOL) return NEWTON_DEFERRED;
   if (n_iter >= MAX_NEWT_ITER) return (errx > MIN_NEWT_TOL) ? 1 : 0;
+  return 0;
+}
+
+// ucon_calc_3vel, phys.c:885-957: u^mu from v^i = u^i/u^t (packed gcov);
+// nonzero when the velocity is not time-like
+__device__ __forceinline__ int ucon_3vel(const double* v, const double* c, double* ucon)
+{
+  const double discr = +c[0] + c[4] * v[1] * v[1] + c[7] * v[2] * v[2] + c[9] * v[3] * v[3] +
+                       2. * (c[1] * v[1] + c[2] * v[2] + c[3] * v[3] + c[5] * v[1] * v[2] + c[6] * v[1] * v[3] +
+                             c[8] * v[2] * v[3]);
+  if (discr > 0.) return 1;
+  ucon[0] = 1. / sqrt(-discr);
+#pragma unroll
+  for (int j = 1; j < 4; j++) ucon[j] = v[j] * ucon[0];
+  return 0;
+}
+
+// Utoprimgen(UEVOLVE) for EOMFFDE, step_ch.c:544-546: UtoU without the
+// rest-mass term (phys.c:228-233) -> Utoprim_ffde, phys.ffde.c:141-372
+// (CHECKBSQMINUSESQ 1, AVOIDUTINF 2): B^i/alpha and B_i/alpha (U2BBsq,
+// 1261-1284), E^i/alpha from B_j x T^t_k (TtoEconOalpha, 1287-1318), the
+// B^2 - E^2 > 0 cap on the drift Lorentz factor, v^i (EBcovtovcon,
+// 551-560), u^i through ucon_calc_3vel (vcon2pr's active branch,
+// transforms.c:372-377, stores u^i).  pr[RHO], pr[UU] keep the guess.
+// Returns 0 or FAIL_FFDE_SPACELIKE.
+__device__ __forceinline__ int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, double gammamax)
+{
+  double U[NPR];
+#pragma unroll
+  for (int k = 0; k < NPR; k++) U[k] = Uin[k] / g.g;
+  const double alphasq = 1. / (-g.gcon[0]);
+  double Bcon[4] = {0.0, U[B1], U[B2], U[B3]}, Bcov[4];
+  lower_v(Bcon, g.gcov, Bcov);
+  double Bsq = 0.0;
+#pragma unroll
+  for (int j = 1; j < 4; j++) Bsq += Bcov[j] * Bcon[j];
+  double o = 1.0 / (Bsq * g.g);
+  double Econ[4], Ecov[4];
+  Econ[0] = 0;
+  Econ[1] = (Bcov[2] * U[U3] - Bcov[3] * U[U2]) * (o);
+  Econ[2] = (Bcov[3] * U[U1] - Bcov[1] * U[U3]) * (o);
+  Econ[3] = (Bcov[1] * U[U2] - Bcov[2] * U[U1]) * (o);
+  double realBsq = Bsq;
+  lower_v(Econ, g.gcov, Ecov);
+  double Esq = 0.0;
+#pragma unroll
+  for (int j = 1; j < 4; j++) Esq += Econ[j] * Ecov[j];
+  const double BsqmEsq = Bsq - Esq;
+  const double gammasq = Bsq / BsqmEsq;
+  if ((gammasq > gammamax * gammamax) || (gammasq < 1.0)) {
+    const double Gsq = 1.0 - 1.0 / (gammamax * gammamax);
+    realBsq = (sqrt(Esq * Bsq / Gsq));
+  }
+  o = 1.0 / (realBsq * g.g);
+  double vcon[4];
+  vcon[0] = 0.;
+  vcon[1] = alphasq * (-g.gcon[1] + (Ecov[2] * Bcov[3] - Ecov[3] * Bcov[2]) * o);
+  vcon[2] = alphasq * (-g.gcon[2] + (Ecov[3] * Bcov[1] - Ecov[1] * Bcov[3]) * o);
+  vcon[3] = alphasq * (-g.gcon[3] + (Ecov[1] * Bcov[2] - Ecov[2] * Bcov[1]) * o);
+  double ucon[4];
+  if (ucon_3vel(vcon, g.gcov, ucon)) return FAIL_FFDE_SPACELIKE;
+  pr[U1] = ucon[1];
+  pr[U2] = ucon[2];
+  pr[U3] = ucon[3];
+  pr[B1] = U[B1];
+  pr[B2] = U[B2];
+  pr[B3] = U[B3];
   return 0;
 }
 

@@ -34,7 +34,10 @@ __host__ __device__ constexpr int conn_plane(int k, int l, int j) { return GEO_C
 struct Params {
   int lim;          // 3 MC, 4 PARA
   int fluxmethod;   // 0 LAXF, 1 HLL
+  int eom;          // 0 GRMHD, 1 FFDE
+  int bc;           // 0 torus (bounds.fishmon.c), 1 rotating star (bounds.ns.c)
   double cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit, tf;
+  double omegastar; // bc 1: angular frequency of the stellar surface
 };
 
 // device-resident scalars of the run (one struct in device memory)
@@ -69,6 +72,7 @@ struct StepArgs {
   double* blockmin;      // per-block dt minima: [2][nblocks]
   double* ubuf;          // 8 planes: conserved state of zones deferred to the tail kernel
   int* worklist;         // deferred zone indices (capacity: one plane)
+  const double* pstep;   // the step's p (the star's inner ghost field is held at it)
   int nblocks_flux;
   DevScalars* sc;
 };
@@ -104,5 +108,18 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 {
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
+
+// launchers of the templated step kernels (harm_step.cu: FP64 instantiations
+// and dispatch; harm_step_mixed.cu: the mixed-precision instantiations)
+void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
+                   const double* pb, double* pf, double c2);
+void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
+void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
+                         const double* pb, double* pf, double c2);
+void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv);
 
 }  // namespace harm

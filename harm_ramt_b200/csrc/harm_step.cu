@@ -25,6 +25,10 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
   const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
   if (i > a.gr.n1 || j > a.gr.n2) return;
   const long long z = a.gr.at(i, j);
+  if (a.pp.eom) {  // the b^2 checks are GRMHD-only (fixup.c:1214-1233)
+    a.bsqf[z] = 0;
+    return;
+  }
   double pr[NPR];
 #pragma unroll
   for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * a.gr.plane + z);
@@ -69,12 +73,14 @@ __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __
 }
 
 // ---------------------------------------------------------------- bounds
-// inflow_check_rel4vel for dir 1 at CENT, fixup.c:1733-1830 (both x1 ends OUTFLOW)
+// inflow_check_rel4vel for dir 1 at CENT, fixup.c:1733-1830: the outer x1
+// end is OUTFLOW for both problems, the inner one only for the torus
 __device__ __forceinline__ int inflow_check_x1(const StepArgs& a, int i, double* pr, const Geo<double>& g)
 {
   double ucon[4];
   ucon_of(pr, g, ucon);
-  const bool dofix = ((i <= -1) && (ucon[1] > 0.)) || ((i >= a.gr.n1) && (ucon[1] < 0.));
+  const bool inner_outflow = (a.pp.bc == 0);
+  const bool dofix = ((i <= -1) && inner_outflow && (ucon[1] > 0.)) || ((i >= a.gr.n1) && (ucon[1] < 0.));
   if (!dofix) return 0;
   double gamma = gamma_of(pr, g);
   pr[U1] /= gamma;
@@ -100,14 +106,57 @@ __device__ __forceinline__ int inflow_check_x1(const StepArgs& a, int i, double*
   return 0;
 }
 
+// x1 ghost zone (i, j) of the rotating star, bounds.ns.c:96-203 (NSSURFACE)
+// and 207-271 (OUTFLOW), EXTRAP 1: densities scaled by sqrt(-g); inside, the
+// velocity of the surface rotating at omegastar (vcon2pr -> ucon_calc_3vel;
+// left as it was if that fails) and the field of the step's p; outside,
+// linear extrapolation factors in x1
+__device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* pv, int i, int j, double* pr)
+{
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  const int ri = (i < 0) ? 0 : a.gr.n1 - 1;
+  const long long zr = a.gr.at(ri, j);
+  const double gr_ = gdet_at(a, CENT, zr), gi = gdet_at(a, CENT, z);
+#pragma unroll
+  for (int k = RHO; k <= UU; k++) pr[k] = pv[k * pl + zr] * gr_ / gi;
+  if (i < 0) {
+    Geo<double> g;
+    load_geo(a, CENT, z, g);
+    const double vcon[4] = {0., 0., 0., a.pp.omegastar};
+    double ucon[4];
+    if (!ucon_3vel(vcon, g.gcov, ucon)) {
+      pr[U1] = ucon[1];
+      pr[U2] = ucon[2];
+      pr[U3] = ucon[3];
+    } else {
+#pragma unroll
+      for (int k = U1; k <= U3; k++) pr[k] = pv[k * pl + z];
+    }
+#pragma unroll
+    for (int k = B1; k <= B3; k++) pr[k] = a.pstep[k * pl + z];
+  } else {
+    const double dx1 = a.pp.dx1;
+    pr[U1] = pv[U1 * pl + zr] * (1. - 2 * (i - ri) * dx1);
+#pragma unroll
+    for (int k = U2; k <= U3; k++) pr[k] = pv[k * pl + zr] * (1. - (i - ri) * dx1);
+    pr[B1] = pv[B1 * pl + zr] * gr_ / gi;
+#pragma unroll
+    for (int k = B2; k <= B3; k++) pr[k] = pv[k * pl + zr] * (1. - (i - ri) * dx1);
+  }
+}
+
 // outflow copy + inflow check + gamma limit of an x1 ghost zone (i, j),
-// bounds.fishmon.c:28-60 and 192-230 (EXTRAP 0)
+// bounds.fishmon.c:28-60 and 192-230 (EXTRAP 0), or the star's
 __device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, int i, int j, double* pr)
 {
-  const int is = (i < 0) ? 0 : a.gr.n1 - 1;
-  const long long zs = a.gr.at(is, j);
+  if (a.pp.bc == 1) {
+    x1_ghost_star(a, pv, i, j, pr);
+  } else {
+    const int is = (i < 0) ? 0 : a.gr.n1 - 1;
+    const long long zs = a.gr.at(is, j);
 #pragma unroll
-  for (int k = 0; k < NPR; k++) pr[k] = pv[k * a.gr.plane + zs];
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * a.gr.plane + zs];
+  }
   Geo<double> g;
   load_geo(a, CENT, a.gr.at(i, j), g);
   int rc = inflow_check_x1(a, i, pr, g);
@@ -115,10 +164,12 @@ __device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, in
   if (rc) report_fail(a.sc, rc, i, j);
 }
 
-// bound_prim (bounds.fishmon.c:14-330) and bound_pflag (boundsint.c:4-60)
-// for every ghost zone; reads only active zones, writes only ghost zones.
-// Polar ghosts of the x1 ghost columns take the x1 ghost value of their
-// mirror row, as the reference's x1-then-x2 order produces.
+// bound_prim (bounds.fishmon.c:14-330 or bounds.ns.c:10-355) and
+// bound_pflag (boundsint.c:4-60) for every ghost zone; reads only active
+// zones, writes only ghost zones.  Polar ghosts of the x1 ghost columns take
+// the x1 ghost value of their mirror row, as the reference's x1-then-x2 order
+// produces.  The torus's POLEDEATH rows are zeroed here for ghost zones and
+// by k_poledeath for the first and last active rows.
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
@@ -129,9 +180,10 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
   if (xin && yin) return;
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
   double pr[NPR];
+  const bool poledeath = (a.pp.bc == 0);
   if (yin) {
     x1_ghost(a, pv, i, j, pr);
-    if (j == 0 || j == n2 - 1) {
+    if (poledeath && (j == 0 || j == n2 - 1)) {
       pr[U2] *= 0.;
       pr[B2] *= 0.;
     }
@@ -144,8 +196,10 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
     } else {
       x1_ghost(a, pv, i, jm, pr);
     }
-    pr[U2] *= 0.;
-    pr[B2] *= 0.;
+    if (poledeath) {
+      pr[U2] *= 0.;
+      pr[B2] *= 0.;
+    }
   }
 #pragma unroll
   for (int k = 0; k < NPR; k++) pv[k * pl + z] = pr[k];
@@ -439,17 +493,16 @@ __global__ void k_planes_to_ref(StepArgs a, const double* __restrict__ pv, doubl
   }
 }
 
-// launchers for the FP64 instantiations (the mixed ones live in harm_step_mixed.cu)
-void launch_flux_mixed(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
-void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
-void launch_update_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
-                         double* pf, double c2);
-void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv);
+// launchers of the templated kernels: the FP64 instantiations here, the
+// mixed-precision ones in harm_step_mixed.cu
 
-void launch_flux(int para, int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
 {
-  if (mixed) launch_flux_mixed(para, g, b, s, a, pb);
-  else if (para) k_flux<double, true, false><<<g, b, 0, s>>>(a, pb);
+  if (mixed) launch_flux_mixed(para, ffde, g, b, s, a, pb);
+  else if (ffde) {
+    if (para) k_flux<double, true, true><<<g, b, 0, s>>>(a, pb);
+    else k_flux<double, false, true><<<g, b, 0, s>>>(a, pb);
+  } else if (para) k_flux<double, true, false><<<g, b, 0, s>>>(a, pb);
   else k_flux<double, false, false><<<g, b, 0, s>>>(a, pb);
 }
 
@@ -459,12 +512,13 @@ void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a)
   else k_emf<double><<<g, b, 0, s>>>(a);
 }
 
-void launch_update(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
-                   double* pf, double c2)
+void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
+                   const double* pb, double* pf, double c2)
 {
-  if (mixed) launch_update_mixed(g, b, s, a, pi, pb, pf, c2);
+  if (mixed) launch_update_mixed(ffde, g, b, s, a, pi, pb, pf, c2);
+  else if (ffde) k_update<double, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
   else k_update<double, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
-  k_update_tail<<<148, 64, 0, s>>>(a, pi, pf);
+  if (!ffde) k_update_tail<<<148, 64, 0, s>>>(a, pi, pf);
 }
 
 void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)

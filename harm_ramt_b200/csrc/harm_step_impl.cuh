@@ -110,7 +110,8 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 
 // fluxcalc for both directions over i in [-1,N1], j in [-1,N2]: x1 faces
 // with i >= 0, x2 faces with j >= 0 (FZLOOP ranges), then the fix_flux
-// rules that do not read another face (fixup.c:1357-1410).  Blocks are
+// rules that do not read another face (fixup.c:1357-1410; the inner x1 mass
+// flux clamp only where that end is OUTFLOW, i.e. for the torus).  Blocks are
 // 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
 // states once: the x1 neighbour's right state arrives by warp shuffle and
 // the x2 neighbour's through shared memory (the first lane/row recomputes).
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(32 * FLUX_BY) k_flux(StepArgs a, const double*
   if (in && i >= 0) {
     face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij);
     dt1 = (dtij < dt1) ? dtij : dt1;
-    if (i == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
+    if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
     if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
 #pragma unroll
     for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
@@ -312,6 +313,16 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
       const double dUr = dU1 + dU2;
       U[k] = 1.0 * U[k] + 0.0 * 0.0 + cdt * (dUr + dUg[k]);
     }
+  }
+  if constexpr (FFDE) {
+    // Utoprim_ffde, then fixup1zone's Lorentz-factor limit (the floors are
+    // GRMHD-only, fixup.c:293); pflag is left as it was
+    int rc = utoprim_ffde(U, g, pfz, a.pp.gammamax);
+    if (!rc) rc = limit_gamma(a.pp.gammamax, pfz, g);
+    if (rc) report_fail(a.sc, rc, i, j);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
+    return;
   }
   int niter;
   int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP);

@@ -8,18 +8,22 @@
 
 namespace harm {
 
-void launch_flux_mixed(int para, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
 {
-  if (para) k_flux<float, true, false><<<g, b, 0, s>>>(a, pb);
+  if (ffde) {
+    if (para) k_flux<float, true, true><<<g, b, 0, s>>>(a, pb);
+    else k_flux<float, false, true><<<g, b, 0, s>>>(a, pb);
+  } else if (para) k_flux<float, true, false><<<g, b, 0, s>>>(a, pb);
   else k_flux<float, false, false><<<g, b, 0, s>>>(a, pb);
 }
 
 void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a) { k_emf<float><<<g, b, 0, s>>>(a); }
 
-void launch_update_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi, const double* pb,
-                         double* pf, double c2)
+void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
+                         const double* pb, double* pf, double c2)
 {
-  k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  if (ffde) k_update<float, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  else k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
 }
 
 void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv) { k_horizon<float><<<1, 1024, 0, s>>>(a, pv); }

@@ -43,8 +43,9 @@ extern "C" {
 #define HARM_ENOMEM 4        /* device allocation failed */
 #define HARM_EGEOMETRY 5     /* geometry tables not symmetric or not uploaded */
 #define HARM_EFAIL 6         /* the step hit a fatal check of the reference
-                                (fail() codes, global.h:562-579); see
-                                harm_status.fail_code */
+                                (fail() codes, global.h:562-579, or 20 when
+                                Utoprim_ffde met a space-like drift velocity,
+                                phys.ffde.c:281-284); see harm_status.fail_code */
 
 /* limiter / Riemann solver / equations of motion (step_ch.h:22-80) */
 #define HARM_LIM_MC 3
@@ -52,6 +53,14 @@ extern "C" {
 #define HARM_FLUX_LAXF 0
 #define HARM_FLUX_HLL 1
 #define HARM_EOM_GRMHD 0
+#define HARM_EOM_FFDE 1      /* force-free electrodynamics (phys.ffde.c) */
+
+/* boundary set of the problem (the bounds*.c plugin) */
+#define HARM_BC_TORUS 0      /* bounds.fishmon.c: OUTFLOW at both x1 ends,
+                                polar mirror with POLEDEATH */
+#define HARM_BC_STAR 1       /* bounds.ns.c: rotating stellar surface inside
+                                (NSSURFACE), extrapolating OUTFLOW outside,
+                                plain polar mirror */
 
 /* arithmetic of the step */
 #define HARM_PREC_FP64 0   /* everything FP64: bit-identical to the reference */
@@ -66,7 +75,7 @@ typedef struct harm_config {
   int n1, n2;           /* interior zones */
   int lim;              /* HARM_LIM_MC or HARM_LIM_PARA */
   int fluxmethod;       /* HARM_FLUX_HLL or HARM_FLUX_LAXF */
-  int eom;              /* HARM_EOM_GRMHD */
+  int eom;              /* HARM_EOM_GRMHD or HARM_EOM_FFDE */
   int precision;        /* HARM_PREC_FP64 or HARM_PREC_MIXED */
   double cour;          /* Courant factor */
   double gam;           /* adiabatic index */
@@ -78,6 +87,9 @@ typedef struct harm_config {
   double bsqorholimit;  /* BSQORHOLIMIT */
   double bsqoulimit;    /* BSQOULIMIT */
   double tf;            /* end time: dt is clamped so that t + dt <= tf */
+  int bc;               /* HARM_BC_TORUS or HARM_BC_STAR */
+  double omegastar;     /* HARM_BC_STAR: angular frequency of the surface
+                           (Omegastar, bounds.ns.c:107) */
 } harm_config;
 
 typedef struct harm_status {

@@ -15,10 +15,11 @@ problem/size pair is its own library: ``libharmref_<problem>_<N1>x<N2>.so``.
 
 Build patches (each one asserted to apply exactly):
   1. mympi.h:15          USEMPI 1 -> 0            (no MPI here; serial oracle)
-  2. global.h:202        EOMTYPE per problem      (EOMGRMHD for the torus)
-  3. metric.h:11         MCOORD per problem       (KSCOORDS for the torus)
+  2. global.h:202        EOMTYPE per problem      (EOMGRMHD torus, EOMFFDE dipole)
+  3. metric.h:11         MCOORD per problem       (KSCOORDS torus, SPCMINKMETRIC dipole)
   4. global.h:126-127    N1, N2 per build
-  5. torus: init.fishmon.c -> init.c, bounds.fishmon.c -> bounds.c
+  5. torus: init.fishmon.c -> init.c, bounds.fishmon.c -> bounds.c;
+     dipole: init.ns.c -> init.c, bounds.ns.c -> bounds.c
   6. gcc >= 10 needs -fcommon (tentative definitions in defs.h)
   7. dudp_calc.c, utoprim_{1d,2d,5d2}_final.c are left out (gcc rejects their
      block-scope static prototypes); they are only reached through the
@@ -63,7 +64,11 @@ init_mpi.c boundmpi.c boundmpiint.c sources.c phys.ffde.c advance.c reconstructe
 
 PROBLEMS = {
     # Fishbone-Moncrief torus in modified Kerr-Schild coordinates (GRMHD).
-    "torus": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c"),
+    "torus": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c", defs=[]),
+    # Force-free aligned rotator (dipole field, rotating stellar surface) in
+    # flat space, spherical polar log-r coordinates (FFDE).
+    "dipole": dict(eom="EOMFFDE", mcoord="SPCMINKMETRIC", init="init.ns.c", bounds="bounds.ns.c",
+                   defs=["-DHR_PROBLEM_DIPOLE"]),
 }
 
 CFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-fPIC", "-w", "-std=gnu99"]
@@ -152,7 +157,7 @@ def build(src, problem, n1, n2, jobs, force=False):
 
     def cc(name):
         obj = os.path.join(bdir, name[:-2] + ".o")
-        cmd = ["gcc"] + CFLAGS + ["-c", os.path.join(bdir, name), "-o", obj]
+        cmd = ["gcc"] + CFLAGS + PROBLEMS[problem]["defs"] + ["-c", os.path.join(bdir, name), "-o", obj]
         r = subprocess.run(cmd, cwd=bdir, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"compile failed: {name}\n{r.stderr[-3000:]}")

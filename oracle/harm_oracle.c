@@ -17,7 +17,11 @@
  * REMOVERESTMASSFROMUU = 1, WHICHEOM = WITHGDET (e = sqrt(-g) for every
  * equation), FLUXB = FLUXCTTOTH with CORNGDETVERSION 1, BDIRCONT 1,
  * TIMEORDER 2 (midpoint RK2), UTOPRIMVERSION 2D, CHECKSOLUTION 1,
- * UTOPRIMADJUST = UTOPRIMAVG, torus boundaries (bounds.fishmon.c).
+ * UTOPRIMADJUST = UTOPRIMAVG.  Physics: EOMGRMHD (Utoprim_2d) or EOMFFDE
+ * (Utoprim_ffde, phys.ffde.c:141-372).  Boundaries: the torus's
+ * (bounds.fishmon.c: OUTFLOW at both x1 ends, polar mirror with POLEDEATH)
+ * or the rotating star's (bounds.ns.c: NSSURFACE inside, extrapolating
+ * OUTFLOW outside, plain polar mirror).
  */
 #include "harm_oracle.h"
 
@@ -62,6 +66,11 @@ enum { FLUX_LAXF = 0, FLUX_HLL = 1 };
 #define FAIL_COEFF_SUP 5
 #define FAIL_UTCALC_DISCR 6
 #define FAIL_VSQ_NEG 9
+/* Utoprim_ffde's space-like velocity (phys.ffde.c:281-284) aborts the step
+   through MYFUN; it has no FAIL_* number in the reference */
+#define FAIL_FFDE_SPACELIKE 20
+
+enum { BC_TORUS = 0, BC_STAR = 1 };
 
 struct ho_state {
   ho_config c;
@@ -71,6 +80,7 @@ struct ho_state {
   double *gammacheck; /* persistent, [n1+2][n2+2] like fixup.c:393 */
   double hz[6];       /* horizon accounting, see ho_get_horizon */
   double dt_free;     /* the last step's next dt before the end-time clamp */
+  const double *pcur; /* the step's p (bounds.ns.c reads the global p's field) */
   long ncb;
   int fail;
 };
@@ -288,13 +298,15 @@ static int limit_gamma(double gammamax, double *pr, const geo *g)
   return 0;
 }
 
-/* inflow_check_rel4vel for dir = 1 at CENT, fixup.c:1733-1830, torus
-   boundaries (both x1 ends OUTFLOW).  Returns a fail code. */
+/* inflow_check_rel4vel for dir = 1 at CENT, fixup.c:1733-1830; the inner
+   x1 end is OUTFLOW for the torus and NSSURFACE (never fixed) for the star,
+   the outer end OUTFLOW for both.  Returns a fail code. */
 static int inflow_check_x1(const ho_state *s, double *pr, const geo *g)
 {
   double ucon[4];
   ucon_of(pr, g, ucon);
-  int dofix = ((g->i <= -1) && (ucon[1] > 0.)) || ((g->i >= s->c.n1) && (ucon[1] < 0.));
+  const int inner_outflow = (s->c.bc == BC_TORUS);
+  int dofix = ((g->i <= -1) && inner_outflow && (ucon[1] > 0.)) || ((g->i >= s->c.n1) && (ucon[1] < 0.));
   if (!dofix) return 0;
   double gamma = gamma_of(pr, g);
   pr[U1] /= gamma;
@@ -436,7 +448,8 @@ static int fluxcalc(ho_state *s, const double *pb, double *F, int dir, double *n
   return 0;
 }
 
-/* fix_flux, fixup.c:1357-1410 (both x2 ends POLARAXIS, both x1 ends OUTFLOW) */
+/* fix_flux, fixup.c:1357-1410 (both x2 ends POLARAXIS; the x1 inner mass
+   flux clamp only where that end is OUTFLOW) */
 static void fix_flux(ho_state *s)
 {
   const int n1 = s->c.n1, n2 = s->c.n2;
@@ -456,8 +469,9 @@ static void fix_flux(ho_state *s)
   for (i = 0; i < n1; i++)
     for (k = 0; k < NPR; k++)
       if (k != U2) P(s->F2, i, j)[k] = 0.;
-  for (j = -1; j < n2; j++)
-    if (P(s->F1, 0, j)[RHO] > 0) P(s->F1, 0, j)[RHO] = 0;
+  if (s->c.bc == BC_TORUS)
+    for (j = -1; j < n2; j++)
+      if (P(s->F1, 0, j)[RHO] > 0) P(s->F1, 0, j)[RHO] = 0;
   for (j = -1; j < n2; j++)
     if (P(s->F1, n1, j)[RHO] < 0) P(s->F1, n1, j)[RHO] = 0;
 }
@@ -574,6 +588,22 @@ static void raise_g(const double *v, const geo *g, double *w)
 
 /* Utoprim_new_body, utoprim_2d.c:128-310.  U and prim in the rescaled form
    of Utoprim_2d.  Returns the pflag code. */
+/* ucon_calc_3vel, phys.c:885-957: u^mu from v^i = u^i/u^t; nonzero when
+   the velocity is not time-like */
+static int ucon_3vel(const double *vcon, const geo *g, double *ucon)
+{
+  double discr = +GCOV(g, 0, 0) + GCOV(g, 1, 1) * vcon[1] * vcon[1] + GCOV(g, 2, 2) * vcon[2] * vcon[2] +
+                 GCOV(g, 3, 3) * vcon[3] * vcon[3] +
+                 2. * (GCOV(g, 0, 1) * vcon[1] + GCOV(g, 0, 2) * vcon[2] + GCOV(g, 0, 3) * vcon[3] +
+                       GCOV(g, 1, 2) * vcon[1] * vcon[2] + GCOV(g, 1, 3) * vcon[1] * vcon[3] +
+                       GCOV(g, 2, 3) * vcon[2] * vcon[3]);
+  int j;
+  if (discr > 0.) return 1;
+  ucon[0] = 1. / sqrt(-discr);
+  for (j = 1; j < 4; j++) ucon[j] = vcon[j] * ucon[0];
+  return 0;
+}
+
 static int u2p_body(const double *U, const geo *g, double *prim, double gam, double gammafail, long *ncb)
 {
   u2pctx c;
@@ -671,6 +701,56 @@ static int utoprimgen(const ho_state *s, const double *U, const geo *g, double *
   return pfl;
 }
 
+/* Utoprimgen(UEVOLVE) for EOMFFDE, step_ch.c:544-546 -> UtoU (phys.c:228-233,
+   no rest-mass term) -> Utoprim_ffde, phys.ffde.c:141-372 with
+   CHECKBSQMINUSESQ 1, AVOIDUTINF 2, REMOVET 0, AVOIDCS 0, FIXB3 0:
+   U2BBsq (1261-1284), TtoEconOalpha (1287-1318), EBcovtovcon (551-560),
+   vcon2pr(VELREL4) (transforms.c:348-393, whose active branch stores
+   u^i) -> ucon_calc_3vel (phys.c:885-957).  diss_account is accounting
+   only.  pr[RHO], pr[UU] keep the guess; pflag is not written. */
+static int utoprim_ffde(const ho_state *s, const double *Uin, const geo *g, double *pr)
+{
+  double U[NPR], Bcon[4], Bcov[4], Econ[4], Ecov[4], T[4], vcon[4];
+  double alphasq, Bsq, Esq, BsqmEsq, realBsq, gammasq, Gsq, o;
+  int j, k;
+  for (k = 0; k < NPR; k++) U[k] = Uin[k] / g->g;
+  alphasq = 1. / (-GCON(g, 0, 0));
+  Bcon[0] = 0.0;
+  for (j = 1; j < 4; j++) Bcon[j] = U[B1 + j - 1];
+  lower_v(Bcon, g, Bcov);
+  Bsq = 0.0;
+  for (j = 1; j < 4; j++) Bsq += Bcov[j] * Bcon[j];
+  for (j = 0; j < 4; j++) T[j] = U[UU + j];
+  o = 1.0 / (Bsq * g->g);
+  Econ[0] = 0;
+  Econ[1] = (Bcov[2] * T[3] - Bcov[3] * T[2]) * (o);
+  Econ[2] = (Bcov[3] * T[1] - Bcov[1] * T[3]) * (o);
+  Econ[3] = (Bcov[1] * T[2] - Bcov[2] * T[1]) * (o);
+  realBsq = Bsq;
+  lower_v(Econ, g, Ecov);
+  Esq = 0.0;
+  for (j = 1; j < 4; j++) Esq += Econ[j] * Ecov[j];
+  BsqmEsq = Bsq - Esq;
+  gammasq = Bsq / BsqmEsq;
+  if ((gammasq > s->c.gammamax * s->c.gammamax) || (gammasq < 1.0)) {
+    Gsq = 1.0 - 1.0 / (s->c.gammamax * s->c.gammamax);
+    realBsq = (sqrt(Esq * Bsq / Gsq));
+  }
+  o = 1.0 / (realBsq * g->g);
+  vcon[1] = alphasq * (-GCON(g, 0, 1) + (Ecov[2] * Bcov[3] - Ecov[3] * Bcov[2]) * o);
+  vcon[2] = alphasq * (-GCON(g, 0, 2) + (Ecov[3] * Bcov[1] - Ecov[1] * Bcov[3]) * o);
+  vcon[3] = alphasq * (-GCON(g, 0, 3) + (Ecov[1] * Bcov[2] - Ecov[2] * Bcov[1]) * o);
+  double ucon[4];
+  if (ucon_3vel(vcon, g, ucon)) return FAIL_FFDE_SPACELIKE;
+  pr[U1] = ucon[1];
+  pr[U2] = ucon[2];
+  pr[U3] = ucon[3];
+  pr[B1] = U[B1];
+  pr[B2] = U[B2];
+  pr[B3] = U[B3];
+  return 0;
+}
+
 /* source -> source_conn, phys.c:475-619 (cooling off, numerical
    connection): dU[UU+l] = e * sum_j sum_k T^j_k Gamma^k_{l j} */
 static void geom_source(const ho_state *s, const double *pb, const geo *g, double *dU)
@@ -689,12 +769,68 @@ static void geom_source(const ho_state *s, const double *pb, const geo *g, doubl
 }
 
 /* ------------------------------------------------------------ boundaries */
+/* bound_prim of the rotating star, bounds.ns.c:10-355 with EXTRAP 1:
+   NSSURFACE inside (densities scaled by sqrt(-g), velocity of a surface
+   rotating at omegastar through vcon2pr, field held at the step's p),
+   extrapolating OUTFLOW outside, plain polar mirror (the "sign flips" are
+   multiplications by 1).  Returns a fail code. */
+static int bound_prims_star(ho_state *s, double *pv)
+{
+  const int n1 = s->c.n1, n2 = s->c.n2;
+  const double dx1 = s->c.dx1;
+  int i, j, k, rc, ri;
+#define GD(i, j) (s->gdet[zid(s, (i), (j)) * 4 + CENT])
+  for (j = 0; j < n2; j++) {
+    ri = 0;
+    for (i = -1; i >= -NG; i--) {
+      for (k = RHO; k <= UU; k++) P(pv, i, j)[k] = P(pv, ri, j)[k] * GD(ri, j) / GD(i, j);
+      double vcon[4] = {0., 0., 0., s->c.omegastar}, ucon[4];
+      geo g = getgeo(s, i, j, CENT);
+      if (!ucon_3vel(vcon, &g, ucon)) {
+        P(pv, i, j)[U1] = ucon[1];
+        P(pv, i, j)[U2] = ucon[2];
+        P(pv, i, j)[U3] = ucon[3];
+      }
+      for (k = B1; k <= B3; k++) P(pv, i, j)[k] = P(s->pcur, i, j)[k];
+    }
+    for (i = -1; i >= -NG; i--) {
+      geo g = getgeo(s, i, j, CENT);
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+    }
+  }
+  for (j = 0; j < n2; j++) {
+    ri = n1 - 1;
+    for (i = n1; i <= n1 - 1 + NG; i++) {
+      for (k = RHO; k <= UU; k++) P(pv, i, j)[k] = P(pv, ri, j)[k] * GD(ri, j) / GD(i, j);
+      P(pv, i, j)[U1] = P(pv, ri, j)[U1] * (1. - 2 * (i - ri) * dx1);
+      for (k = U2; k <= U3; k++) P(pv, i, j)[k] = P(pv, ri, j)[k] * (1. - (i - ri) * dx1);
+      P(pv, i, j)[B1] = P(pv, ri, j)[B1] * GD(ri, j) / GD(i, j);
+      for (k = B2; k <= B3; k++) P(pv, i, j)[k] = P(pv, ri, j)[k] * (1. - (i - ri) * dx1);
+    }
+    for (i = n1; i <= n1 - 1 + NG; i++) {
+      geo g = getgeo(s, i, j, CENT);
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+    }
+  }
+#undef GD
+  for (i = -NG; i <= n1 - 1 + NG; i++)
+    for (j = -NG; j <= -1; j++)
+      for (k = 0; k < NPR; k++) P(pv, i, j)[k] = P(pv, i, -j - 1)[k];
+  for (i = -NG; i <= n1 - 1 + NG; i++)
+    for (j = n2; j <= n2 - 1 + NG; j++)
+      for (k = 0; k < NPR; k++) P(pv, i, j)[k] = P(pv, i, 2 * n2 - 1 - j)[k];
+  return 0;
+}
+
 /* bound_prim, bounds.fishmon.c:14-330 with EXTRAP 0, POSDEFMETRIC 0 and
-   POLEDEATH 1.  Returns a fail code. */
+   POLEDEATH 1 (the torus), or the rotating star's.  Returns a fail code. */
 static int bound_prims(ho_state *s, double *pv)
 {
   const int n1 = s->c.n1, n2 = s->c.n2;
   int i, j, k, rc;
+  if (s->c.bc == BC_STAR) return bound_prims_star(s, pv);
   for (j = 0; j < n2; j++) {
     for (i = -1; i >= -NG; i--)
       for (k = 0; k < NPR; k++) P(pv, i, j)[k] = P(pv, 0, j)[k];
@@ -759,6 +895,11 @@ static void bsqflags(ho_state *s, const double *pv, int *pf)
       ostate q;
       const double *pr = P(pv, i, j);
       int f0, f3;
+      if (s->c.eom) { /* the b^2 checks are GRMHD-only (fixup.c:1214-1233) */
+        FL(pf, i, j)[F_BSQORHO] = 0;
+        FL(pf, i, j)[F_BSQOU] = 0;
+        continue;
+      }
       state_of(pr, &g, &q);
       double bsq = dot4(q.bcon, q.bcov);
       if (bsq / pr[RHO] > s->c.bsqorholimit) f0 = 2;
@@ -900,12 +1041,16 @@ static int advance(ho_state *s, const double *pi, const double *pb, double *pf, 
       }
       for (k = 0; k < NPR; k++) ul[k] = Uf[k] = CUf[0] * Ui[k] + CUf[1] * ul[k] + CUf[2] * dt * (dUr[k] + dUg[k]);
       for (k = 0; k < NPR; k++) un[k] += Cunew[0] * Ui[k] + Cunew[1] * dt * (dUr[k] + dUg[k]) + Cunew[2] * Uf[k];
-      int pfl = utoprimgen(s, last ? un : Uf, &g, pfz, &s->ncb);
-      FL(pflag, i, j)[F_FAIL] = pfl;
-      /* fixup1zone, fixup.c:274-377 */
-      const double *fl = s->floors + zid(s, i, j) * 2;
-      if (fl[0] > pfz[RHO]) pfz[RHO] = fl[0];
-      if (fl[1] > pfz[UU]) pfz[UU] = fl[1];
+      if (s->c.eom) {
+        if ((rc = utoprim_ffde(s, last ? un : Uf, &g, pfz))) return rc;
+      } else {
+        int pfl = utoprimgen(s, last ? un : Uf, &g, pfz, &s->ncb);
+        FL(pflag, i, j)[F_FAIL] = pfl;
+        /* fixup1zone, fixup.c:274-377 (floors are GRMHD-only, 293) */
+        const double *fl = s->floors + zid(s, i, j) * 2;
+        if (fl[0] > pfz[RHO]) pfz[RHO] = fl[0];
+        if (fl[1] > pfz[UU]) pfz[UU] = fl[1];
+      }
       if ((rc = limit_gamma(s->c.gammamax, pfz, &g))) return rc;
       for (k = 0; k < NPR; k++) P(pf, i, j)[k] = pfz[k];
     }
@@ -957,7 +1102,11 @@ void ho_destroy(ho_state *s)
   free(s);
 }
 
-void ho_bound(ho_state *s, double *prims) { bound_prims(s, prims); }
+void ho_bound(ho_state *s, double *prims)
+{
+  s->pcur = prims;
+  bound_prims(s, prims);
+}
 void ho_bsqflags(ho_state *s, const double *prims, int *pflag) { bsqflags(s, prims, pflag); }
 
 void ho_get_fluxes(const ho_state *s, double *f1, double *f2)
@@ -1020,6 +1169,7 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
   static const double Cunew[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 1.0}};
   double ndt = 0.0;
   int to, rc, moved;
+  s->pcur = p;
   for (to = 0; to < 2; to++) {
     const double *pi = p;
     const double *pb = (to == 0) ? p : s->pk0;

@@ -28,6 +28,8 @@ typedef struct {
   double cour, gam, dx1, dx2;
   double safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit;
   double tf;
+  int bc;              /* 0 = torus (bounds.fishmon.c), 1 = rotating star (bounds.ns.c) */
+  double omegastar;    /* bc 1: angular frequency of the stellar surface */
 } ho_config;
 
 typedef struct ho_state ho_state;

@@ -46,6 +46,7 @@ void hr_configure(int lim_, int flux_, int timeorder_, double cour_, int rescale
 extern int hr_orig_init_grid(void);
 extern int hr_orig_init_global(void);
 
+#ifndef HR_PROBLEM_DIPOLE
 /* init.fishmon.c:35 with the benchmark's coordinates: plain MKS (defcoord 0),
    R0 = 0, Rout = 40, hslope = 0.3, Rin = 0.98 r_h (initbase.c:103-114). */
 int init_grid(void)
@@ -59,10 +60,29 @@ int init_grid(void)
   Rin = 0.98 * Rhor;
   return 0;
 }
+#else
+/* init.ns.c:62 turned into the force-free aligned rotator: flat space in
+   spherical polar coordinates (MCOORD SPCMINKMETRIC), log-r and uniform
+   theta (defcoord 6, coord.c:283-286), r in [1, 100] stellar radii. */
+static double hr_omegastar = 0.2;
+void hr_set_omegastar(double w) { hr_omegastar = w; }
+double hr_get_omegastar(void) { return Omegastar; }
+int init_grid(void)
+{
+  hr_orig_init_grid();
+  a = 0.0;
+  defcoord = 6;
+  R0 = 0.0;
+  Rin = 1.0;
+  Rout = 100.0;
+  Rhor = rhor_calc(0);
+  return 0;
+}
+#endif
 
-/* init.fishmon.c:61 (ranc(7) seed, gamma, boundary types) plus the
-   algorithm knobs of the benchmark.  Output cadences are pushed out of
-   range; dumps are disabled below. */
+/* init.fishmon.c:61 / init.ns.c:105 (ranc(7) seed, gamma, boundary types)
+   plus the algorithm knobs of the benchmark.  Output cadences are pushed
+   out of range; dumps are disabled below. */
 int init_global(void)
 {
   hr_orig_init_global();
@@ -77,6 +97,9 @@ int init_global(void)
   tf = hr_tf;
   DTd = DTavg = DTener = DTi = DTdebug = 1.0e30;
   DTr = 1000000000L;
+#ifdef HR_PROBLEM_DIPOLE
+  Omegastar = hr_omegastar; /* stellar surface rotation (bounds.ns.c:107) */
+#endif
   return 0;
 }
 

@@ -26,7 +26,8 @@ class OracleConfig(ctypes.Structure):
                 ("eom", ctypes.c_int), ("cour", ctypes.c_double), ("gam", ctypes.c_double), ("dx1", ctypes.c_double),
                 ("dx2", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
                 ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
-                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double)]
+                ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
+                ("omegastar", ctypes.c_double)]
 
 
 def build_oracle(force=False):
@@ -76,10 +77,11 @@ class Oracle:
     """The C restatement run on given geometry and state."""
 
     def __init__(self, n1, n2, geom, *, lim=3, fluxmethod=1, cour=0.8, gam=4.0 / 3.0, dx1, dx2, safe=1.3,
-                 defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1e30):
+                 defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1e30, eom=0,
+                 bc=0, omegastar=0.0):
         self.lib = oracle_lib()
-        self.cfg = OracleConfig(n1, n2, lim, fluxmethod, 0, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                                bsqorholimit, bsqoulimit, tf)
+        self.cfg = OracleConfig(n1, n2, lim, fluxmethod, eom, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+                                bsqorholimit, bsqoulimit, tf, bc, omegastar)
         self.geom = {k: np.ascontiguousarray(geom[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "conn",
                                                                                      "floors")}
         g = self.geom
@@ -158,6 +160,10 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     lib.hr_get_geometry(V(geom["gcov"]), V(geom["gcon"]), V(geom["gdet"]), V(geom["conn"]))
     lib.hr_get_floors(V(geom["floors"]))
     scal0 = s.copy()
+    extra = {"eomtype": lib.hr_eomtype()}
+    if hasattr(lib, "hr_get_omegastar"):
+        lib.hr_get_omegastar.restype = ctypes.c_double
+        extra["omegastar"] = lib.hr_get_omegastar()
     ps, pfs, ts, hz = [], [], [], []
     for n in range(nsteps + 1):
         p = np.zeros((m1, m2, 8))
@@ -182,7 +188,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     lib.hr_get_fluxes(V(f1), V(f2))
     with open(outpath, "wb") as f:
         pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, horizon=hz, F1=f1, F2=f2,
-                         ncyclebreak=lib.hr_get_ncyclebreak()), f, protocol=4)
+                         ncyclebreak=lib.hr_get_ncyclebreak(), **extra), f, protocol=4)
 
 
 def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800):

@@ -34,3 +34,34 @@ def test_oracle_matches_reference(n, lim, flux, nsteps):
     # the run exercised the Newton cycle break (the reference's count is
     # cumulative from init, the oracle's from this run)
     assert r["ncyclebreak"] >= o.ncyclebreak()
+
+
+# force-free aligned rotator (phys.ffde.c, bounds.ns.c): n1 x n2 grid,
+# limiter, flux, steps
+DIPOLE_CASES = [(32, 16, 3, 0, 300), (32, 16, 4, 1, 150), (64, 32, 3, 1, 40)]
+
+
+@pytest.mark.parametrize("n1,n2,lim,flux,nsteps", DIPOLE_CASES)
+def test_oracle_matches_reference_dipole_ffde(n1, n2, lim, flux, nsteps):
+    r = ht.ref_run(n1, n2, lim=lim, flux=flux, nsteps=nsteps, problem="dipole")
+    if r is None:
+        pytest.skip("reference build (oracle/_ref) of the dipole problem not present")
+    assert r["eomtype"] == 1
+    o = ht.Oracle(n1, n2, r["geom"], lim=lim, fluxmethod=flux, eom=1, bc=1, omegastar=r["omegastar"],
+                  **ht.ref_config(r))
+    p = r["prims"][0].copy()
+    f = r["pflag"][0].copy()
+    t, dt = r["times"][0]
+    for s in range(1, nsteps + 1):
+        rc, t, dt = o.step(p, f, t, dt)
+        assert rc == 0
+        assert np.array_equal(p, r["prims"][s]), f"step {s}: primitives differ"
+        assert np.array_equal(f[..., 0], r["pflag"][s][..., 0]), f"step {s}: flags differ"
+        assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
+        assert np.array_equal(o.horizon(), r["horizon"][s]), f"step {s}: surface accounting differs"
+    f1, f2 = o.fluxes()
+    I = ht.interior
+    assert np.array_equal(I(f1), I(r["F1"])) and np.array_equal(I(f2), I(r["F2"]))
+    # force-free state: no matter, field held fixed inside the star's surface
+    assert not p[..., 0:2].any()
+    assert np.array_equal(p[:3, 3:-3, 5:8], r["prims"][0][:3, 3:-3, 5:8])
