@@ -57,7 +57,7 @@ class _Config(ctypes.Structure):
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
                 ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
                 ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
-                ("omegastar", ctypes.c_double)]
+                ("omegastar", ctypes.c_double), ("currents", ctypes.c_int)]
 
 
 class _Status(ctypes.Structure):
@@ -80,7 +80,7 @@ _lib = None
 EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
            "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
-           "harm_kernel_name", "harm_get_horizon", "harm_set_end_time"]
+           "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents"]
 
 
 def load_library(path=None):
@@ -120,6 +120,7 @@ def load_library(path=None):
     lib.harm_torus_init.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
     lib.harm_profile_step.argtypes = [vp, dp, ip, ctypes.c_int]
     lib.harm_get_horizon.argtypes = [vp, dp]
+    lib.harm_get_currents.argtypes = [vp, dp, dp, dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
     if path is None:
@@ -184,13 +185,13 @@ class HarmGPU:
 
     def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
-                 precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0):
+                 precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0, currents=False):
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
         self.safe = safe
         cfg = _Config(n1, n2, lim, fluxmethod, eom, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                      bsqorholimit, bsqoulimit, tf, bc, omegastar)
+                      bsqorholimit, bsqoulimit, tf, bc, omegastar, int(bool(currents)))
         h = ctypes.c_void_p()
         _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
         self._h = h
@@ -280,7 +281,7 @@ class HarmGPU:
 
     def profile_step(self):
         """One step with a CUDA event after every kernel: {name: (ms, launches)}."""
-        nk = 13
+        nk = 15
         ms = np.zeros(nk)
         n = np.zeros(nk, dtype=np.int32)
         _check(self.lib.harm_profile_step(self._h, _dp(ms), _ip(n), nk), "harm_profile_step")
@@ -293,6 +294,15 @@ class HarmGPU:
         out = np.zeros(6)
         _check(self.lib.harm_get_horizon(self._h, _dp(out)), "harm_get_horizon")
         return dict(zip(("pdot_rho", "pdot_uu", "em_bsq_term", "em_bb_term", "pcum_rho", "pcum_uu"), out.tolist()))
+
+    def get_currents(self):
+        """(jcon [n1m,n2m,4], fcon [n1m,n2m,6], cfaraday [n1m,n2m,5,3]) of a
+        context created with currents=True (phys.c:1124-1455 layouts)."""
+        jc = np.zeros((self.n1m, self.n2m, 4))
+        fc = np.zeros((self.n1m, self.n2m, 6))
+        cf = np.zeros((self.n1m, self.n2m, 5, 3))
+        _check(self.lib.harm_get_currents(self._h, _dp(jc), _dp(fc), _dp(cf)), "harm_get_currents")
+        return jc, fc, cf
 
     def get_fluxes(self):
         f1 = np.zeros((self.n1m, self.n2m, NPR))

@@ -26,6 +26,9 @@ __global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
 __global__ void k_fixup_compute(StepArgs a, const double* pv);
 __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd);
 __global__ void k_dt_finalize(StepArgs a);
+__global__ void k_faraday(StepArgs a, const double* pv);
+__global__ void k_current(StepArgs a);
+__global__ void k_currents_commit(StepArgs a);
 __global__ void k_ref_to_planes(StepArgs a, const double* ref, const int* refflag, double* pv);
 __global__ void k_planes_to_ref(StepArgs a, const double* pv, double* ref, int* refflag);
 }  // namespace harm
@@ -40,7 +43,7 @@ struct harm_ctx {
   Grid gr;
   int n1m, n2m;
   // device buffers
-  double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin, *d_ubuf;
+  double *d_p, *d_pk0, *d_geo, *d_F1, *d_F2, *d_emf, *d_gammacheck, *d_fixbuf, *d_blockmin, *d_ubuf, *d_cur;
   float* d_geo32;
   int *d_pflag, *d_worklist;
   double* d_stage;   // reference-layout prims staging buffer
@@ -86,6 +89,8 @@ struct harm_ctx {
     a.ubuf = d_ubuf;
     a.worklist = d_worklist;
     a.pstep = d_p;
+    a.cur = d_cur;
+    a.pp.currents = cfg.currents;
     a.nblocks_flux = nblocks_flux;
     a.sc = d_sc;
     return a;
@@ -105,10 +110,11 @@ static dim3 grid2(int ni, int nj, dim3 b) { return dim3((ni + b.x - 1) / b.x, (n
 
 // kernel classes of one step, in launch order (for per-kernel timing)
 enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_CHECKSOL, KC_CHECKSERIAL, KC_FIXC,
-       KC_FIXA, KC_DT, KC_HORIZON, KC_COUNT };
+       KC_FIXA, KC_DT, KC_HORIZON, KC_FARADAY, KC_CURRENT, KC_COUNT };
 static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", "k_update", "k_bound", "k_poledeath",
                                                "k_gammacheck", "k_checksol", "k_checksol_serial", "k_fixup_compute",
-                                               "k_fixup_apply", "k_dt_finalize", "k_horizon"};
+                                               "k_fixup_apply", "k_dt_finalize", "k_horizon", "k_faraday",
+                                               "k_current"};
 
 struct Timer {
   // records an event after every launch when active
@@ -176,6 +182,14 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
       k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
       T.mark(s, KC_POLE);
     }
+  }
+  if (c->cfg.currents) {
+    // step_ch.c:143-156: Faraday slots and J^mu at the new time
+    k_faraday<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, c->d_p);
+    T.mark(s, KC_FARADAY);
+    k_current<<<grid2(n1 + 2 * NG - 2, n2 + 2 * NG - 2, b), b, 0, s>>>(a);
+    k_currents_commit<<<1, 1, 0, s>>>(a);
+    T.mark(s, KC_CURRENT);
   }
   launch_horizon(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
   T.mark(s, KC_HORIZON);
@@ -249,6 +263,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   ok &= cudaMalloc(&c->d_sc, sizeof(DevScalars)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_ubuf, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_worklist, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
+  if (cfg->currents) ok &= cudaMalloc(&c->d_cur, (size_t)CUR_NPLANES * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_stage, (size_t)c->n1m * c->n2m * NPR * sizeof(double)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_stagef, (size_t)c->n1m * c->n2m * 5 * sizeof(int)) == cudaSuccess;
   if (!ok) {
@@ -267,6 +282,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   cudaMemsetAsync(c->d_bsqf, 0, (size_t)c->gr.plane, c->stream);
   cudaMemsetAsync(c->d_chk, 0, 2 * (size_t)c->gr.plane, c->stream);
   cudaMemsetAsync(c->d_sc, 0, sizeof(DevScalars), c->stream);
+  if (c->d_cur) cudaMemsetAsync(c->d_cur, 0, (size_t)CUR_NPLANES * pd, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     harm_destroy(c);
     return HARM_ECUDA;
@@ -298,6 +314,7 @@ void harm_destroy(harm_ctx* c)
   cudaFree(c->d_sc);
   cudaFree(c->d_ubuf);
   cudaFree(c->d_worklist);
+  cudaFree(c->d_cur);
   cudaFree(c->d_stage);
   cudaFree(c->d_stagef);
   delete c;
@@ -404,6 +421,17 @@ int harm_set_time(harm_ctx* c, double t, double dt, long long realnstep)
   h.dt_free = dt;
   h.realnstep = realnstep;
   CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  if (c->cfg.currents) {
+    // the t = 0 evaluation of initbase.c:653-658 on the uploaded state, from
+    // cleared slots (the reference's arrays start at zero)
+    const StepArgs a = c->args();
+    const dim3 b(32, 4);
+    CK(cudaMemsetAsync(c->d_cur, 0, (size_t)CUR_NPLANES * c->gr.plane * sizeof(double), c->stream));
+    k_faraday<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, c->stream>>>(a, c->d_p);
+    k_current<<<grid2(c->cfg.n1 + 2 * NG - 2, c->cfg.n2 + 2 * NG - 2, b), b, 0, c->stream>>>(a);
+    k_currents_commit<<<1, 1, 0, c->stream>>>(a);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(c->stream));
   return HARM_OK;
 }
@@ -472,6 +500,35 @@ int harm_sync(harm_ctx* c, harm_status* st)
     st->newton_iters = h.newton_iters;
   }
   return h.status ? HARM_EFAIL : HARM_OK;
+}
+
+int harm_get_currents(harm_ctx* c, double* jcon, double* fcon, double* cfaraday)
+{
+  if (!c) return HARM_EINVAL;
+  if (!c->cfg.currents) return HARM_EINVAL;
+  const long long pl = c->gr.plane;
+  std::vector<double> h((size_t)CUR_NPLANES * pl);
+  DevScalars sc;
+  CK(cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(h.data(), c->d_cur, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // reference slots: 0 = newest F^{it}, 4 = the previous, 3 = two back
+  const int lev[5] = {sc.cur_ring, -1, -1, (sc.cur_ring + 1) % 3, (sc.cur_ring + 2) % 3};
+  for (int ii = 0; ii < c->n1m; ii++)
+    for (int jj = 0; jj < c->n2m; jj++) {
+      const long long zd = (long long)jj * c->gr.pitch + ii, zr = (long long)ii * c->n2m + jj;
+      if (jcon)
+        for (int k = 0; k < 4; k++) jcon[zr * 4 + k] = h[(CUR_JCON + k) * pl + zd];
+      if (fcon)
+        for (int k = 0; k < 6; k++) fcon[zr * 6 + k] = h[(CUR_FCON + k) * pl + zd];
+      if (cfaraday)
+        for (int sl = 0; sl < 5; sl++)
+          for (int k = 0; k < 3; k++) {
+            const int plane = (sl == 1) ? CUR_S1 + k : (sl == 2) ? CUR_S2 + k : CUR_RING + 3 * lev[sl] + k;
+            cfaraday[(zr * 5 + sl) * 3 + k] = h[plane * pl + zd];
+          }
+    }
+  return HARM_OK;
 }
 
 int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)
@@ -587,6 +644,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   if (cfg->lim != HARM_LIM_MC && cfg->lim != HARM_LIM_PARA) return HARM_EINVAL;
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
   if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
+  if (cfg->currents) return HARM_EINVAL;  // the diagnostic currents need a context
   harm_ctx c;
   memset(&c, 0, sizeof(c));
   c.cfg = *cfg;

@@ -35,6 +35,7 @@ struct Params {
   int lim;          // 3 MC, 4 PARA
   int fluxmethod;   // 0 LAXF, 1 HLL
   int eom;          // 0 GRMHD, 1 FFDE
+  int currents;     // 1: Faraday slots and J^mu every step
   int bc;           // 0 torus (bounds.fishmon.c), 1 rotating star (bounds.ns.c)
   double cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit, tf;
   double omegastar; // bc 1: angular frequency of the stellar surface
@@ -54,6 +55,9 @@ struct DevScalars {
   double hz[6];          // horizon accounting of the last step (see k_horizon)
   int ndeferred;         // zones whose inversion went to the tail kernel (this substep)
   int ndeferred_total;   // same, summed since the last harm_set_time
+  int cur_ring;          // currents: ring level holding the newest F^{i t}
+  long long ccalls;      // currents: calls of current_calc_1 (its static count)
+  double clastdt;        // currents: dt of the previous call (its static lastdt)
 };
 
 struct StepArgs {
@@ -73,6 +77,7 @@ struct StepArgs {
   double* ubuf;          // 8 planes: conserved state of zones deferred to the tail kernel
   int* worklist;         // deferred zone indices (capacity: one plane)
   const double* pstep;   // the step's p (the star's inner ghost field is held at it)
+  double* cur;           // currents (25 planes): F^{i t} ring 3x3, F^{i r} 3, F^{i h} 3, fcon 6, jcon 4
   int nblocks_flux;
   DevScalars* sc;
 };
@@ -108,6 +113,9 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 {
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
+
+// plane offsets of the currents block
+constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 21, CUR_NPLANES = 25;
 
 // launchers of the templated step kernels (harm_step.cu: FP64 instantiations
 // and dispatch; harm_step_mixed.cu: the mixed-precision instantiations)

@@ -451,6 +451,98 @@ __global__ void k_dt_finalize(StepArgs a)
   }
 }
 
+// ---------------------------------------------------------------- currents
+// current_doprecalc(0..3, p) with WHICHCURRENTCALC 1 (phys.c:1124-1218): at
+// every zone centre (ghosts included) the F^{i t} components go to the next
+// level of a three-level ring (the reference shifts slot 0 -> 4 -> 3), F^{i r}
+// and F^{i h} to their slots, and the six F^{mu nu} to fcon.
+__global__ void k_faraday(StepArgs a, const double* __restrict__ pv)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
+  if (i >= a.gr.n1 + NG || j >= a.gr.n2 + NG) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  double pr[NPR];
+#pragma unroll
+  for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * pl + z);
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  State<double> q;
+  state_of(pr, g, q);
+  const double* b = q.bcov;
+  const double* u = q.ucov;
+  double* c = a.cur + z;
+  const int lv = (a.sc->cur_ring + 1) % 3;
+  c[(CUR_RING + 3 * lv + 0) * pl] = -1.0 / g.g * (-b[3] * u[2] + b[2] * u[3]);
+  c[(CUR_RING + 3 * lv + 1) * pl] = -1.0 / g.g * (b[3] * u[1] - b[1] * u[3]);
+  c[(CUR_RING + 3 * lv + 2) * pl] = -1.0 / g.g * (-b[2] * u[1] + b[1] * u[2]);
+  c[(CUR_S1 + 0) * pl] = -1.0 / g.g * (b[3] * u[2] - b[2] * u[3]);
+  c[(CUR_S1 + 1) * pl] = -1.0 / g.g * (-b[3] * u[0] + b[0] * u[3]);
+  c[(CUR_S1 + 2) * pl] = -1.0 / g.g * (b[2] * u[0] - b[0] * u[2]);
+  c[(CUR_S2 + 0) * pl] = -1.0 / g.g * (-b[3] * u[1] + b[1] * u[3]);
+  c[(CUR_S2 + 1) * pl] = -1.0 / g.g * (b[3] * u[0] - b[0] * u[3]);
+  c[(CUR_S2 + 2) * pl] = -1.0 / g.g * (-b[1] * u[0] + b[0] * u[1]);
+  c[(CUR_FCON + 0) * pl] = -1.0 / g.g * (b[3] * u[2] - b[2] * u[3]);
+  c[(CUR_FCON + 1) * pl] = -1.0 / g.g * (-b[3] * u[1] + b[1] * u[3]);
+  c[(CUR_FCON + 2) * pl] = -1.0 / g.g * (b[2] * u[1] - b[1] * u[2]);
+  c[(CUR_FCON + 3) * pl] = -1.0 / g.g * (b[3] * u[0] - b[0] * u[3]);
+  c[(CUR_FCON + 4) * pl] = -1.0 / g.g * (-b[2] * u[0] + b[0] * u[2]);
+  c[(CUR_FCON + 5) * pl] = -1.0 / g.g * (b[1] * u[0] - b[0] * u[1]);
+}
+
+// current_calc_1, phys.c:1335-1455, over i in [-2, N1+2), j in [-2, N2+2):
+// J^mu = (1/g) d_nu (g F^{mu nu}) with centred space differences and, from the
+// third call on, the one-sided second-order time derivative through the three
+// ring levels (dt of this step and of the previous call).  J^h's x1 difference
+// takes g at i-1 from the zone itself, as the reference's geomr does.
+__global__ void k_current(StepArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - (NG - 1);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - (NG - 1);
+  if (i >= a.gr.n1 + NG - 1 || j >= a.gr.n2 + NG - 1) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  const long long zrp = a.gr.at(i + 1, j), zrm = a.gr.at(i - 1, j), zhp = a.gr.at(i, j + 1), zhm = a.gr.at(i, j - 1);
+  const DevScalars* sc = a.sc;
+  const int ln = (sc->cur_ring + 1) % 3, l0 = sc->cur_ring, l3 = (sc->cur_ring + 2) % 3;
+  const double dtl = sc->clastdt, dtr = sc->dt;
+  const double idx1 = 1.0 / (2.0 * a.pp.dx1), idx2 = 1.0 / (2.0 * a.pp.dx2);
+  const double gt = gdet_at(a, CENT, z), grp = gdet_at(a, CENT, zrp), grm = gdet_at(a, CENT, zrm);
+  const double ghp = gdet_at(a, CENT, zhp), ghm = gdet_at(a, CENT, zhm);
+  const double* c = a.cur;
+#define S1(zz, k) c[(CUR_S1 + (k)) * pl + (zz)]
+#define S2(zz, k) c[(CUR_S2 + (k)) * pl + (zz)]
+  double* J = a.cur + CUR_JCON * pl + z;
+  J[0] = 1. / gt * (grp * S1(zrp, 0) - grm * S1(zrm, 0)) * idx1 + 1. / gt * (ghp * S2(zhp, 0) - ghm * S2(zhm, 0)) * idx2;
+  double d[3] = {0., 0., 0.};
+  const bool timed = sc->ccalls >= 2;
+  if (timed) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double fl = c[(CUR_RING + 3 * l3 + k) * pl + z], f0 = c[(CUR_RING + 3 * l0 + k) * pl + z];
+      const double fr = c[(CUR_RING + 3 * ln + k) * pl + z];
+      const double AA = (dtr * (fl - f0) + dtl * (fr - f0)) / (dtl * dtr * (dtl + dtr));
+      const double BB = (-dtr * dtr * (fl - f0) + dtl * dtl * (fr - f0)) / (dtl * dtr * (dtl + dtr));
+      d[k] = 2.0 * AA * dtr + BB;
+    }
+  }
+  // the reference adds the integer 0 where there is no time derivative
+  J[pl] = (timed ? d[0] : 0.) + 1. / gt * (ghp * S2(zhp, 1) - ghm * S2(zhm, 1)) * idx2;
+  J[2 * pl] = (timed ? d[1] : 0.) + 1. / gt * (grp * S1(zrp, 1) - gt * S1(zrm, 1)) * idx1;
+  J[3 * pl] = (timed ? d[2] : 0.) + 1. / gt * (grp * S1(zrp, 2) - grm * S1(zrm, 2)) * idx1 +
+              1. / gt * (ghp * S2(zhp, 2) - ghm * S2(zhm, 2)) * idx2;
+#undef S1
+#undef S2
+}
+
+// the statics of current_calc_1 (calls, lastdt) and the ring's newest level
+__global__ void k_currents_commit(StepArgs a)
+{
+  DevScalars* s = a.sc;
+  s->cur_ring = (s->cur_ring + 1) % 3;
+  s->ccalls += 1;
+  s->clastdt = s->dt;
+}
+
 // ---------------------------------------------------------------- layouts
 // Reference layout (defs.h: zone (ii, jj) at ii*n2m + jj, components
 // fastest) <-> the step's planes.  Threads run along the planes' fast index

@@ -90,6 +90,9 @@ typedef struct harm_config {
   int bc;               /* HARM_BC_TORUS or HARM_BC_STAR */
   double omegastar;     /* HARM_BC_STAR: angular frequency of the surface
                            (Omegastar, bounds.ns.c:107) */
+  int currents;         /* 1: the diagnostic currents J^mu and the Faraday
+                           tensor F^{mu nu} every step, as step_ch.c:143-156
+                           does (WHICHCURRENTCALC 1); 0: not computed */
 } harm_config;
 
 typedef struct harm_status {
@@ -154,10 +157,19 @@ int harm_get_fluxes(harm_ctx* ctx, double* F1, double* F2);
    (sum of pdot * dt since harm_set_time). */
 int harm_get_horizon(harm_ctx* ctx, double* out);
 
+/* Diagnostic currents of a context created with currents = 1, in the
+   reference's layouts (phys.c:1124-1455): jcon [n1m][n2m][4] (J^mu at zone
+   centres, the outermost ghost ring left 0), fcon [n1m][n2m][6]
+   (F^{tr}, F^{th}, F^{tp}, F^{rh}, F^{rp}, F^{hp}), cfaraday
+   [n1m][n2m][5][3] (the five time/space slots of current_precalc); any
+   pointer may be NULL.  harm_set_time() performs the t = 0 evaluation of
+   initbase.c:653-658 on the uploaded state. */
+int harm_get_currents(harm_ctx* ctx, double* jcon, double* fcon, double* cfaraday);
+
 /* Diagnostics: runs one step outside the graph with a CUDA event after
    every kernel and returns, per kernel class (harm_kernel_name(k), k <
    HARM_NKERNELS), the summed device time in ms and the launch count. */
-#define HARM_NKERNELS 13
+#define HARM_NKERNELS 15
 int harm_profile_step(harm_ctx* ctx, double* ms, int* launches, int nclasses);
 const char* harm_kernel_name(int k);
 

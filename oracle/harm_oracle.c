@@ -81,6 +81,11 @@ struct ho_state {
   double hz[6];       /* horizon accounting, see ho_get_horizon */
   double dt_free;     /* the last step's next dt before the end-time clamp */
   const double *pcur; /* the step's p (bounds.ns.c reads the global p's field) */
+  double *cfar;       /* current_precalc slots, [n1m][n2m][5][3] like cfaraday */
+  double *fcon;       /* [n1m][n2m][6] */
+  double *jcon;       /* [n1m][n2m][4] */
+  long ccalls;        /* current_calc_1's static call count */
+  double clastdt;     /* and its static lastdt */
   long ncb;
   int fail;
 };
@@ -1058,6 +1063,104 @@ static int advance(ho_state *s, const double *pi, const double *pb, double *pf, 
   return 0;
 }
 
+/* ------------------------------------------------------------ currents */
+/* current_doprecalc(0..3, p) with WHICHCURRENTCALC 1 (phys.c:1124-1218,
+   all at CENT over FULLLOOP): slot 3 <- 4 <- 0 and the new f^{it} in slot
+   0, f^{ir} in 1, f^{ih} in 2, and fcon (the six f^{mu nu}). */
+static void currents_precalc(ho_state *s, const double *p)
+{
+  const int n1 = s->c.n1, n2 = s->c.n2;
+  int i, j, c;
+  for (i = -NG; i <= n1 - 1 + NG; i++)
+    for (j = -NG; j <= n2 - 1 + NG; j++) {
+      geo g = getgeo(s, i, j, CENT);
+      ostate q;
+      const double *b, *u;
+      double *f = s->cfar + zid(s, i, j) * 15, *fc = s->fcon + zid(s, i, j) * 6;
+      state_of(P(p, i, j), &g, &q);
+      b = q.bcov;
+      u = q.ucov;
+      for (c = 0; c < 3; c++) {
+        f[3 * 3 + c] = f[4 * 3 + c];
+        f[4 * 3 + c] = f[0 * 3 + c];
+      }
+      f[0] = -1.0 / g.g * (-b[3] * u[2] + b[2] * u[3]);
+      f[1] = -1.0 / g.g * (b[3] * u[1] - b[1] * u[3]);
+      f[2] = -1.0 / g.g * (-b[2] * u[1] + b[1] * u[2]);
+      f[3] = -1.0 / g.g * (b[3] * u[2] - b[2] * u[3]);
+      f[4] = -1.0 / g.g * (-b[3] * u[0] + b[0] * u[3]);
+      f[5] = -1.0 / g.g * (b[2] * u[0] - b[0] * u[2]);
+      f[6] = -1.0 / g.g * (-b[3] * u[1] + b[1] * u[3]);
+      f[7] = -1.0 / g.g * (b[3] * u[0] - b[0] * u[3]);
+      f[8] = -1.0 / g.g * (-b[1] * u[0] + b[0] * u[1]);
+      fc[0] = -1.0 / g.g * (b[3] * u[2] - b[2] * u[3]);
+      fc[1] = -1.0 / g.g * (-b[3] * u[1] + b[1] * u[3]);
+      fc[2] = -1.0 / g.g * (b[2] * u[1] - b[1] * u[2]);
+      fc[3] = -1.0 / g.g * (b[3] * u[0] - b[0] * u[3]);
+      fc[4] = -1.0 / g.g * (-b[2] * u[0] + b[0] * u[2]);
+      fc[5] = -1.0 / g.g * (b[1] * u[0] - b[0] * u[1]);
+    }
+}
+
+/* current_calc_1, phys.c:1335-1455: J^mu = (1/g) d_nu (g F^{mu nu}) with
+   centred space differences over LOOPP11 x LOOPP12 and, from the third call
+   on, a second-order one-sided time derivative through the last three
+   slots.  J^h's x1 difference uses the zone's own g at i-1 (geomr), as the
+   reference does. */
+static void currents_calc(ho_state *s, double dt)
+{
+  const int n1 = s->c.n1, n2 = s->c.n2;
+  const double dtl = s->clastdt, dtr = dt;
+  const double idx1 = 1.0 / (2.0 * s->c.dx1), idx2 = 1.0 / (2.0 * s->c.dx2);
+  int i, j;
+#define GC(i, j) (s->gdet[zid(s, (i), (j)) * 4 + CENT])
+#define CF(i, j, slot, c) (s->cfar[zid(s, (i), (j)) * 15 + (slot) * 3 + (c)])
+  for (i = -NG + 1; i < n1 + NG - 1; i++)
+    for (j = -NG + 1; j < n2 + NG - 1; j++) {
+      double *J = s->jcon + zid(s, i, j) * 4;
+      const double gt = GC(i, j), grp = GC(i + 1, j), ghp = GC(i, j + 1), grm = GC(i - 1, j), ghm = GC(i, j - 1);
+      J[0] = 1. / gt * (grp * CF(i + 1, j, 1, 0) - grm * CF(i - 1, j, 1, 0)) * idx1 +
+             1. / gt * (ghp * CF(i, j + 1, 2, 0) - ghm * CF(i, j - 1, 2, 0)) * idx2;
+      if (s->ccalls >= 2) {
+        double d[3];
+        int c;
+        for (c = 0; c < 3; c++) {
+          double fl = CF(i, j, 3, c), f0 = CF(i, j, 4, c), fr = CF(i, j, 0, c);
+          double AA = (dtr * (fl - f0) + dtl * (fr - f0)) / (dtl * dtr * (dtl + dtr));
+          double BB = (-dtr * dtr * (fl - f0) + dtl * dtl * (fr - f0)) / (dtl * dtr * (dtl + dtr));
+          d[c] = 2.0 * AA * dtr + BB;
+        }
+        J[1] = d[0] + 1. / gt * (ghp * CF(i, j + 1, 2, 1) - ghm * CF(i, j - 1, 2, 1)) * idx2;
+        J[2] = d[1] + 1. / gt * (grp * CF(i + 1, j, 1, 1) - gt * CF(i - 1, j, 1, 1)) * idx1;
+        J[3] = d[2] + 1. / gt * (grp * CF(i + 1, j, 1, 2) - grm * CF(i - 1, j, 1, 2)) * idx1 +
+               1. / gt * (ghp * CF(i, j + 1, 2, 2) - ghm * CF(i, j - 1, 2, 2)) * idx2;
+      } else {
+        J[1] = 0 + 1. / gt * (ghp * CF(i, j + 1, 2, 1) - ghm * CF(i, j - 1, 2, 1)) * idx2;
+        J[2] = 0 + 1. / gt * (grp * CF(i + 1, j, 1, 1) - gt * CF(i - 1, j, 1, 1)) * idx1;
+        J[3] = 0 + 1. / gt * (grp * CF(i + 1, j, 1, 2) - grm * CF(i - 1, j, 1, 2)) * idx1 +
+               1. / gt * (ghp * CF(i, j + 1, 2, 2) - ghm * CF(i, j - 1, 2, 2)) * idx2;
+      }
+    }
+#undef GC
+#undef CF
+  s->ccalls++;
+  s->clastdt = dt;
+}
+
+void ho_init_currents(ho_state *s, const double *p, double dt)
+{
+  currents_precalc(s, p);
+  currents_calc(s, dt);
+}
+
+void ho_get_currents(const ho_state *s, double *jcon, double *fcon, double *cfaraday)
+{
+  const size_t nz = (size_t)s->n1m * s->n2m;
+  if (jcon) memcpy(jcon, s->jcon, nz * 4 * sizeof(double));
+  if (fcon) memcpy(fcon, s->fcon, nz * 6 * sizeof(double));
+  if (cfaraday) memcpy(cfaraday, s->cfar, nz * 15 * sizeof(double));
+}
+
 /* ------------------------------------------------------------ public */
 ho_state *ho_create(const ho_config *cfg, const double *gcov, const double *gcon, const double *gdet, const double *conn,
                     const double *floors)
@@ -1084,6 +1187,9 @@ ho_state *ho_create(const ho_config *cfg, const double *gcov, const double *gcon
   s->ulast = (double *)calloc(nz * NPR, sizeof(double));
   s->unew = (double *)calloc(nz * NPR, sizeof(double));
   s->gammacheck = (double *)calloc((size_t)(cfg->n1 + 2) * (cfg->n2 + 2), sizeof(double));
+  s->cfar = (double *)calloc(nz * 15, sizeof(double));
+  s->fcon = (double *)calloc(nz * 6, sizeof(double));
+  s->jcon = (double *)calloc(nz * 4, sizeof(double));
   return s;
 }
 
@@ -1099,6 +1205,7 @@ void ho_destroy(ho_state *s)
   if (!s) return;
   free(s->pk0); free(s->dq); free(s->pl); free(s->pr); free(s->F1); free(s->F2);
   free(s->emf); free(s->prc); free(s->ulast); free(s->unew); free(s->gammacheck);
+  free(s->cfar); free(s->fcon); free(s->jcon);
   free(s);
 }
 
@@ -1183,6 +1290,9 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
       if ((rc = fixup_utoprim(s, pf, pflag))) return rc;
     if ((rc = bound_prims(s, pf))) return rc;
   }
+  /* step_ch.c:143-156: Faraday slots and currents at the new time */
+  currents_precalc(s, p);
+  currents_calc(s, *dt);
   horizon_flux(s, p, *dt);
   moved = *dt > 0.;
   *t += *dt;

@@ -60,6 +60,13 @@ void ho_get_fluxes(const ho_state *s, double *f1, double *f2);
    pcum[X1DN][RHO], pcum[X1DN][UU] (cumulative since creation) */
 void ho_get_horizon(const ho_state *s, double *out);
 
+/* diagnostic currents, WHICHCURRENTCALC 1: ho_init_currents() is the t = 0
+   call of initbase.c:653-658 on the initial state; every ho_step() then
+   updates them as step_ch.c:143-156 does.  jcon [n1m][n2m][4], fcon
+   [n1m][n2m][6], cfaraday [n1m][n2m][5][3] (any may be NULL). */
+void ho_init_currents(ho_state *s, const double *p, double dt);
+void ho_get_currents(const ho_state *s, double *jcon, double *fcon, double *cfaraday);
+
 /* count of Newton cycle-break events since creation */
 long ho_ncyclebreak(const ho_state *s);
 

@@ -197,6 +197,15 @@ void hr_get_fluxes(double *f1, double *f2)
   memcpy(f2, &a_F2[0][0][0], sizeof(a_F2));
 }
 
+/* diagnostic currents (phys.c:1124-1455): jcon [N1M][N2M][4], fcon
+   [N1M][N2M][6], cfaraday [N1M][N2M][5][3] */
+void hr_get_currents(double *jcon_, double *fcon_, double *cfaraday_)
+{
+  memcpy(jcon_, &a_jcon[0][0][0], sizeof(a_jcon));
+  memcpy(fcon_, &a_fcon[0][0][0], sizeof(a_fcon));
+  memcpy(cfaraday_, &a_cfaraday[0][0][0][0], sizeof(a_cfaraday));
+}
+
 /* gcov/gcon [N1M][N2M][4 loc][4][4], gdet [N1M][N2M][4], conn [N1M][N2M][4][4][4] */
 void hr_get_geometry(double *gcov_, double *gcon_, double *gdet_, double *conn_)
 {

@@ -57,6 +57,10 @@ def oracle_lib():
         lib.ho_step.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int), dp, dp]
         lib.ho_bound.argtypes = [vp, dp]
         lib.ho_set_end_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp]
+        lib.ho_init_currents.argtypes = [vp, dp, ctypes.c_double]
+        lib.ho_init_currents.restype = None
+        lib.ho_get_currents.argtypes = [vp, dp, dp, dp]
+        lib.ho_get_currents.restype = None
         lib.ho_set_end_time.restype = None
         lib.ho_bsqflags.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_int)]
         lib.ho_get_fluxes.argtypes = [vp, dp, dp]
@@ -93,6 +97,15 @@ class Oracle:
         if getattr(self, "h", None):
             self.lib.ho_destroy(self.h)
             self.h = None
+
+    def init_currents(self, p, dt):
+        self.lib.ho_init_currents(self.h, _dp(np.ascontiguousarray(p)), dt)
+
+    def currents(self):
+        jc, fc, cf = np.zeros((self.n1m, self.n2m, 4)), np.zeros((self.n1m, self.n2m, 6)), np.zeros(
+            (self.n1m, self.n2m, 5, 3))
+        self.lib.ho_get_currents(self.h, _dp(jc), _dp(fc), _dp(cf))
+        return jc, fc, cf
 
     def set_end_time(self, tf, t, dt):
         """moves the end time; returns the re-clamped dt"""
@@ -164,7 +177,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     if hasattr(lib, "hr_get_omegastar"):
         lib.hr_get_omegastar.restype = ctypes.c_double
         extra["omegastar"] = lib.hr_get_omegastar()
-    ps, pfs, ts, hz = [], [], [], []
+    ps, pfs, ts, hz, cur = [], [], [], [], []
     for n in range(nsteps + 1):
         p = np.zeros((m1, m2, 8))
         pf = np.zeros((m1, m2, 5), dtype=np.int32)
@@ -177,6 +190,9 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
         h6 = np.zeros(6)
         lib.hr_get_horizon(V(h6))
         hz.append(h6)
+        jc, fc, cf = np.zeros((m1, m2, 4)), np.zeros((m1, m2, 6)), np.zeros((m1, m2, 5, 3))
+        lib.hr_get_currents(V(jc), V(fc), V(cf))
+        cur.append((jc, fc, cf))
         if n < nsteps:
             os.dup2(devnull, 2)
             rcs = lib.hr_step(1)
@@ -188,6 +204,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     lib.hr_get_fluxes(V(f1), V(f2))
     with open(outpath, "wb") as f:
         pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, horizon=hz, F1=f1, F2=f2,
+                         currents=cur,
                          ncyclebreak=lib.hr_get_ncyclebreak(), **extra), f, protocol=4)
 
 

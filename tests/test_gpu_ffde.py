@@ -14,11 +14,11 @@ import harmtest as ht
 pytestmark = pytest.mark.gpu
 
 
-def _gpu(harm, r, lim, flux, precision=0):
+def _gpu(harm, r, lim, flux, precision=0, currents=False):
     n1, n2 = r["n1"], r["n2"]
     cfg = ht.ref_config(r)
     h = harm.HarmGPU(n1, n2, cfg.pop("dx1"), cfg.pop("dx2"), lim=lim, fluxmethod=flux, eom=harm.EOM_FFDE,
-                     bc=harm.BC_STAR, omegastar=r["omegastar"], precision=precision, **cfg)
+                     bc=harm.BC_STAR, omegastar=r["omegastar"], precision=precision, currents=currents, **cfg)
     g = r["geom"]
     h.upload_geometry(g["gcov"], g["gcon"], g["gdet"], g["conn"], g["floors"])
     h.set_prims(r["prims"][0], r["pflag"][0])
@@ -36,7 +36,7 @@ def _ref(n1, n2, lim, flux, nsteps):
 @pytest.mark.parametrize("lim,flux,nsteps", [(3, 0, 60), (4, 1, 40)])
 def test_ffde_gpu_matches_reference_dipole(harm, lim, flux, nsteps):
     r = _ref(32, 16, lim, flux, nsteps)
-    h = _gpu(harm, r, lim, flux)
+    h = _gpu(harm, r, lim, flux, currents=True)
     for s in range(1, nsteps + 1):
         h.step_ch(1)
         st = h.sync()
@@ -45,6 +45,7 @@ def test_ffde_gpu_matches_reference_dipole(harm, lim, flux, nsteps):
         assert np.array_equal(fg[..., 0], r["pflag"][s][..., 0])
         assert (st["t"], st["dt"]) == tuple(r["times"][s])
         assert list(h.get_horizon().values()) == list(r["horizon"][s]), f"step {s}: surface accounting"
+        assert all(np.array_equal(x, y) for x, y in zip(h.get_currents(), r["currents"][s])), f"step {s}: currents"
     f1g, f2g = h.get_fluxes()
     I = ht.interior
     assert np.array_equal(I(f1g), I(r["F1"])) and np.array_equal(I(f2g), I(r["F2"]))

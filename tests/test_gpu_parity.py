@@ -92,7 +92,9 @@ def test_gpu_matches_reference_torus32(harm):
     if r is None:
         pytest.skip("reference build (oracle/_ref) not present")
     cfg = ht.ref_config(r)
+    cfg["currents"] = True
     h = _gpu_from(harm, 32, r["geom"], r["prims"][0], r["pflag"][0], r["times"][0][0], r["times"][0][1], 3, 1, cfg)
+    assert all(np.array_equal(x, y) for x, y in zip(h.get_currents(), r["currents"][0])), "t=0 currents"
     for s in range(1, 26):
         h.step_ch(1)
         st = h.sync()
@@ -100,6 +102,9 @@ def test_gpu_matches_reference_torus32(harm):
         _assert_same(I(pg), fg, I(r["prims"][s]), r["pflag"][s], f"step {s}")
         assert (st["t"], st["dt"]) == tuple(r["times"][s])
         assert list(h.get_horizon().values()) == list(r["horizon"][s]), f"step {s}: horizon accounting"
+        jc, fc, cf = h.get_currents()
+        rj, rf, rc = r["currents"][s]
+        assert np.array_equal(jc, rj) and np.array_equal(fc, rf) and np.array_equal(cf, rc), f"step {s}: currents"
 
 
 @pytest.mark.slow

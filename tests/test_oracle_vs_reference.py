@@ -19,6 +19,8 @@ def test_oracle_matches_reference(n, lim, flux, nsteps):
     p = r["prims"][0].copy()
     f = r["pflag"][0].copy()
     t, dt = r["times"][0]
+    o.init_currents(p, dt)
+    assert all(np.array_equal(x, y) for x, y in zip(o.currents(), r["currents"][0])), "t=0 currents differ"
     nfixed = 0
     for s in range(1, nsteps + 1):
         rc, t, dt = o.step(p, f, t, dt)
@@ -27,6 +29,7 @@ def test_oracle_matches_reference(n, lim, flux, nsteps):
         assert np.array_equal(f[3:-3, 3:-3, 0], r["pflag"][s][3:-3, 3:-3, 0]), f"step {s}: flags differ"
         assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
         assert np.array_equal(o.horizon(), r["horizon"][s]), f"step {s}: horizon accounting differs"
+        assert all(np.array_equal(x, y) for x, y in zip(o.currents(), r["currents"][s])), f"step {s}: currents"
         nfixed += int((f[3:-3, 3:-3, 0] == -1).sum())
     f1, f2 = o.fluxes()
     I = ht.interior
@@ -52,10 +55,12 @@ def test_oracle_matches_reference_dipole_ffde(n1, n2, lim, flux, nsteps):
     p = r["prims"][0].copy()
     f = r["pflag"][0].copy()
     t, dt = r["times"][0]
+    o.init_currents(p, dt)
     for s in range(1, nsteps + 1):
         rc, t, dt = o.step(p, f, t, dt)
         assert rc == 0
         assert np.array_equal(p, r["prims"][s]), f"step {s}: primitives differ"
+        assert all(np.array_equal(x, y) for x, y in zip(o.currents(), r["currents"][s])), f"step {s}: currents"
         assert np.array_equal(f[..., 0], r["pflag"][s][..., 0]), f"step {s}: flags differ"
         assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
         assert np.array_equal(o.horizon(), r["horizon"][s]), f"step {s}: surface accounting differs"
