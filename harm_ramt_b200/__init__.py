@@ -24,7 +24,7 @@ import numpy as np
 
 __all__ = ["HarmGPU", "HarmError", "torus_params", "torus_geometry", "torus_init", "load_library", "LIB_PATH",
            "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "PREC_FP64", "PREC_MIXED", "EOM_GRMHD", "EOM_FFDE",
-           "BC_TORUS", "BC_STAR", "NG", "NPR", "pinned_empty", "torus_context"]
+           "BC_TORUS", "BC_STAR", "NG", "NPR", "pinned_empty", "torus_context", "torus_dump_coords"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libharm_b200.so")
 NG = 3
@@ -60,6 +60,12 @@ class _Config(ctypes.Structure):
                 ("omegastar", ctypes.c_double), ("currents", ctypes.c_int)]
 
 
+class _DumpHeader(ctypes.Structure):
+    _fields_ = [("startx1", ctypes.c_double), ("startx2", ctypes.c_double), ("a", ctypes.c_double),
+                ("R0", ctypes.c_double), ("Rin", ctypes.c_double), ("Rout", ctypes.c_double),
+                ("hslope", ctypes.c_double), ("defcoord", ctypes.c_int)]
+
+
 class _Status(ctypes.Structure):
     _fields_ = [("fail_code", ctypes.c_int), ("fail_i", ctypes.c_int), ("fail_j", ctypes.c_int),
                 ("fixups", ctypes.c_int), ("realnstep", ctypes.c_longlong), ("t", ctypes.c_double),
@@ -80,7 +86,8 @@ _lib = None
 EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
            "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
-           "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents"]
+           "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
+           "harm_torus_dump_coords"]
 
 
 def load_library(path=None):
@@ -121,6 +128,8 @@ def load_library(path=None):
     lib.harm_profile_step.argtypes = [vp, dp, ip, ctypes.c_int]
     lib.harm_get_horizon.argtypes = [vp, dp]
     lib.harm_get_currents.argtypes = [vp, dp, dp, dp]
+    lib.harm_write_dump.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(_DumpHeader), dp]
+    lib.harm_torus_dump_coords.argtypes = [ctypes.POINTER(_TorusParams), ctypes.POINTER(_DumpHeader), dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
     if path is None:
@@ -304,6 +313,17 @@ class HarmGPU:
         _check(self.lib.harm_get_currents(self._h, _dp(jc), _dp(fc), _dp(cf)), "harm_get_currents")
         return jc, fc, cf
 
+    def write_dump(self, path, header, coords):
+        """The reference's text dump file of the device state (dump.c).
+        header: dict of startx1, startx2, a, R0, Rin, Rout, hslope, defcoord;
+        coords: [n1m, n2m, 4] X1, X2, r, th at zone centres.  Needs
+        currents=True."""
+        h = _DumpHeader(**{k: header[k] for k in ("startx1", "startx2", "a", "R0", "Rin", "Rout", "hslope",
+                                                   "defcoord")})
+        co = np.ascontiguousarray(coords, dtype=np.float64)
+        assert co.shape == (self.n1m, self.n2m, 4)
+        _check(self.lib.harm_write_dump(self._h, os.fsencode(path), ctypes.byref(h), _dp(co)), "harm_write_dump")
+
     def get_fluxes(self):
         f1 = np.zeros((self.n1m, self.n2m, NPR))
         f2 = np.zeros((self.n1m, self.n2m, NPR))
@@ -318,6 +338,15 @@ def pinned_empty(shape, dtype=np.float64):
     t = torch.empty(tuple(shape), dtype={np.float64: torch.float64, np.int32: torch.int32}[np.dtype(dtype).type],
                     pin_memory=True)
     return t.numpy()
+
+
+def torus_dump_coords(params):
+    """(header dict, coords [n1m, n2m, 4]) of the torus grid for write_dump()."""
+    lib = load_library()
+    h = _DumpHeader()
+    co = np.zeros((params.n1 + 2 * NG, params.n2 + 2 * NG, 4))
+    _check(lib.harm_torus_dump_coords(ctypes.byref(params), ctypes.byref(h), _dp(co)), "harm_torus_dump_coords")
+    return {k: getattr(h, k) for k, _ in _DumpHeader._fields_}, co
 
 
 def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, precision=PREC_FP64, tf=1.0e30,

@@ -11,6 +11,10 @@
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/harm_b200.h"
@@ -29,6 +33,8 @@ __global__ void k_dt_finalize(StepArgs a);
 __global__ void k_faraday(StepArgs a, const double* pv);
 __global__ void k_current(StepArgs a);
 __global__ void k_currents_commit(StepArgs a);
+__global__ void k_dump_columns(StepArgs a, const double* pv, double* out, int* nfail);
+constexpr int DUMP_DYNCOLS = 50;
 __global__ void k_ref_to_planes(StepArgs a, const double* ref, const int* refflag, double* pv);
 __global__ void k_planes_to_ref(StepArgs a, const double* pv, double* ref, int* refflag);
 }  // namespace harm
@@ -529,6 +535,75 @@ int harm_get_currents(harm_ctx* c, double* jcon, double* fcon, double* cfaraday)
           }
     }
   return HARM_OK;
+}
+
+int harm_write_dump(harm_ctx* c, const char* path, const harm_dump_header* hdr, const double* coords)
+{
+  if (!c || !path || !hdr || !coords || !c->cfg.currents) return HARM_EINVAL;
+  const int n1 = c->cfg.n1, n2 = c->cfg.n2;
+  const size_t nz = (size_t)n1 * n2;
+  double* d_out = nullptr;
+  int* d_nf = nullptr;
+  CK(cudaMalloc(&d_out, nz * DUMP_DYNCOLS * sizeof(double)));
+  if (cudaMalloc(&d_nf, sizeof(int)) != cudaSuccess) {
+    cudaFree(d_out);
+    return HARM_ENOMEM;
+  }
+  std::vector<double> cols(nz * DUMP_DYNCOLS);
+  DevScalars sc;
+  int nf = 0;
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  cudaError_t e = cudaMemsetAsync(d_nf, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess) {
+    k_dump_columns<<<grid2(n1, n2, b), b, 0, c->stream>>>(a, c->d_p, d_out, d_nf);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(cols.data(), d_out, cols.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nf, d_nf, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&sc, c->d_sc, sizeof(sc), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_out);
+  cudaFree(d_nf);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "harm_b200: harm_write_dump: %s\n", cudaGetErrorString(e));
+    return HARM_ECUDA;
+  }
+  if (nf) return HARM_EFAIL;
+  FILE* f = fopen(path, "wt");
+  if (!f) return HARM_EINVAL;
+  fprintf(f,
+          "%21.15g %d %d %21.15g %21.15g %21.15g %21.15g %ld %21.15g %21.15g %21.15g %21.15g %21.15g %21.15g %21.15g "
+          "%d\n",
+          sc.t, n1, n2, hdr->startx1, hdr->startx2, c->cfg.dx1, c->cfg.dx2, (long)sc.realnstep, c->cfg.gam, hdr->a,
+          hdr->R0, hdr->Rin, hdr->Rout, hdr->hslope, sc.dt, hdr->defcoord);
+  // rows formatted in parallel chunks, written in order
+  const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::string> chunk(nth);
+  std::vector<std::thread> th;
+  const int n2m = n2 + 2 * NG;
+  for (int t = 0; t < nth; t++)
+    th.emplace_back([&, t]() {
+      const size_t lo = nz * t / nth, hi = nz * (t + 1) / nth;
+      std::string& s = chunk[t];
+      s.reserve((hi - lo) * 56 * 22 + 16);
+      char buf[64];
+      for (size_t zz = lo; zz < hi; zz++) {
+        const int j = (int)(zz / n1), i = (int)(zz % n1);
+        const double* xr = coords + ((size_t)(i + NG) * n2m + (j + NG)) * 4;
+        const double head[6] = {(double)i, (double)j, xr[0], xr[1], xr[2], xr[3]};
+        for (int k = 0; k < 6; k++) s.append(buf, snprintf(buf, sizeof(buf), "%21.15g ", head[k]));
+        const double* v = cols.data() + zz * DUMP_DYNCOLS;
+        for (int k = 0; k < DUMP_DYNCOLS; k++) s.append(buf, snprintf(buf, sizeof(buf), "%21.15g ", v[k]));
+        s.push_back('\n');
+      }
+    });
+  for (auto& x : th) x.join();
+  bool ok = true;
+  for (auto& s : chunk) ok &= fwrite(s.data(), 1, s.size(), f) == s.size();
+  ok &= fclose(f) == 0;
+  return ok ? HARM_OK : HARM_EINVAL;
 }
 
 int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)

@@ -543,6 +543,109 @@ __global__ void k_currents_commit(StepArgs a)
   s->clastdt = s->dt;
 }
 
+// ---------------------------------------------------------------- dumps
+// The dynamic columns of dump_content, dump.c:87-191, for the active zone
+// (i, j) at row j*N1 + i (DUMPLOOP order, global.h:1047): p (8), divb
+// (SETFDIVBFLUXCT, global.h:1152-1180), u^mu, u_mu, b^mu, b_mu, vmin/vmax in
+// x1 and x2 (vchar), sqrt(-g), J^mu, J_mu, F^{mu nu} (6), F_{mu nu} (6
+// through lowerf, phys.c:655-689): DUMP_DYNCOLS values.  A vchar failure
+// (the reference's FAILSTATEMENT) is counted in *nfail.
+constexpr int DUMP_DYNCOLS = 50;
+__global__ void k_dump_columns(StepArgs a, const double* __restrict__ pv, double* __restrict__ out, int* nfail)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (i >= n1 || j >= n2) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  double* o = out + ((long long)j * n1 + i) * DUMP_DYNCOLS;
+  double pr[NPR];
+#pragma unroll
+  for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  State<double> q;
+  state_of(pr, g, q);
+  double vmax1, vmin1, vmax2, vmin2;
+  int rc = vchar_of(pr, q, 1, g, a.pp.gam, vmax1, vmin1);
+  if (!rc) rc = vchar_of(pr, q, 2, g, a.pp.gam, vmax2, vmin2);
+  if (rc) {
+    atomicAdd(nfail, 1);
+    vmax1 = vmin1 = vmax2 = vmin2 = 0.;
+  }
+  // divb (FLUXCT form); 0 on the first active row and at j = N2
+  double divb = 0.;
+  if (j != 0 && j != n2) {
+    const long long z10 = a.gr.at(i - 1, j), z01 = a.gr.at(i, j - 1), z11 = a.gr.at(i - 1, j - 1);
+    const double g00 = gdet_at(a, CENT, z), g10 = gdet_at(a, CENT, z10), g01 = gdet_at(a, CENT, z01);
+    const double g11 = gdet_at(a, CENT, z11);
+    const double b1_00 = pv[B1 * pl + z] * g00, b1_01 = pv[B1 * pl + z01] * g01, b1_10 = pv[B1 * pl + z10] * g10;
+    const double b1_11 = pv[B1 * pl + z11] * g11;
+    const double b2_00 = pv[B2 * pl + z] * g00, b2_10 = pv[B2 * pl + z10] * g10, b2_01 = pv[B2 * pl + z01] * g01;
+    const double b2_11 = pv[B2 * pl + z11] * g11;
+    const double dx1 = a.pp.dx1, dx2 = a.pp.dx2;
+    const double mx = (dx1 > dx2) ? dx1 : dx2;
+    const double num = 0.5 * (b1_00 + b1_01 - b1_10 - b1_11) / dx1 + 0.5 * (b2_00 + b2_10 - b2_01 - b2_11) / dx2;
+    const double den = gdet_at(a, CORN, z) * 0.125 *
+                       fabs(fabs(b1_00 + b1_01 + b1_10 + b1_11 + b2_00 + b2_10 + b2_01 + b2_11) + 1.e-20);
+    divb = fabs(mx * num / den);
+  }
+  int c = 0;
+#pragma unroll
+  for (int k = 0; k < NPR; k++) o[c++] = pr[k];
+  o[c++] = divb;
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = q.ucon[k];
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = q.ucov[k];
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = q.bcon[k];
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = q.bcov[k];
+  o[c++] = vmin1;
+  o[c++] = vmax1;
+  o[c++] = vmin2;
+  o[c++] = vmax2;
+  o[c++] = g.g;
+  double jc[4], jv[4], fc[6];
+#pragma unroll
+  for (int k = 0; k < 4; k++) jc[k] = a.cur[(CUR_JCON + k) * pl + z];
+#pragma unroll
+  for (int k = 0; k < 6; k++) fc[k] = a.cur[(CUR_FCON + k) * pl + z];
+  lower_v(jc, g.gcov, jv);
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = jc[k];
+#pragma unroll
+  for (int k = 0; k < 4; k++) o[c++] = jv[k];
+#pragma unroll
+  for (int k = 0; k < 6; k++) o[c++] = fc[k];
+  // lowerf: F_{jk} = sum_{jp,kp} F^{jp kp} g_{j jp} g_{k kp}, summed in the
+  // reference's loop order from 0, for the six upper-triangle pairs
+  double F[4][4];
+  F[0][0] = F[1][1] = F[2][2] = F[3][3] = 0;
+  F[0][1] = fc[0];
+  F[0][2] = fc[1];
+  F[0][3] = fc[2];
+  F[1][2] = fc[3];
+  F[1][3] = fc[4];
+  F[2][3] = fc[5];
+  F[1][0] = -fc[0];
+  F[2][0] = -fc[1];
+  F[3][0] = -fc[2];
+  F[2][1] = -fc[3];
+  F[3][1] = -fc[4];
+  F[3][2] = -fc[5];
+  const int pj[6] = {0, 0, 0, 1, 1, 2}, pk[6] = {1, 2, 3, 2, 3, 3};
+#pragma unroll
+  for (int m = 0; m < 6; m++) {
+    double s = 0;
+#pragma unroll
+    for (int jp = 0; jp < 4; jp++)
+#pragma unroll
+      for (int kp = 0; kp < 4; kp++) s += F[jp][kp] * g.gcov[sym(pj[m], jp)] * g.gcov[sym(pk[m], kp)];
+    o[c++] = s;
+  }
+}
+
 // ---------------------------------------------------------------- layouts
 // Reference layout (defs.h: zone (ii, jj) at ii*n2m + jj, components
 // fastest) <-> the step's planes.  Threads run along the planes' fast index

@@ -408,6 +408,43 @@ int harm_torus_geometry(const harm_torus_params* P, double* gcov, double* gcon, 
 // init() of initbase.c:297-562 with init.fishmon.c's torus, up to (but not
 // including) the final fixup/bound: the caller applies harm_torus_finish()
 // or uploads and lets the device bound it.
+int harm_torus_dump_coords(const harm_torus_params* P, harm_dump_header* hdr, double* coords)
+{
+  if (!P || !hdr || !coords) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG;
+  Coords c;
+  c.a = P->a;
+  c.R0 = 0.0;
+  const double rhor = 1. + 1 * sqrt(1. - c.a * c.a);
+  c.Rin = P->rin_over_rhor * rhor;
+  c.Rout = P->rout;
+  c.hslope = P->hslope;
+  c.startx1 = log(c.Rin - c.R0);
+  c.startx2 = 0.;
+  c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / n1;
+  c.dx2 = 1. / n2;
+  hdr->startx1 = c.startx1;
+  hdr->startx2 = c.startx2;
+  hdr->a = c.a;
+  hdr->R0 = c.R0;
+  hdr->Rin = c.Rin;
+  hdr->Rout = c.Rout;
+  hdr->hslope = c.hslope;
+  hdr->defcoord = 0;
+  for (int i = -NG; i < n1 + NG; i++)
+    for (int j = -NG; j < n2 + NG; j++) {
+      double X[4], r, th;
+      coord_of(c, i, j, CENT, X);
+      bl_of(c, X, &r, &th);
+      double* o = coords + ((long long)(i + NG) * n2m + (j + NG)) * 4;
+      o[0] = X[1];
+      o[1] = X[2];
+      o[2] = r;
+      o[3] = th;
+    }
+  return HARM_OK;
+}
+
 int harm_torus_init(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet, double* prims)
 {
   if (!P || !gcov || !gcon || !gdet || !prims) return HARM_EINVAL;

@@ -166,6 +166,27 @@ int harm_get_horizon(harm_ctx* ctx, double* out);
    initbase.c:653-658 on the uploaded state. */
 int harm_get_currents(harm_ctx* ctx, double* jcon, double* fcon, double* cfaraday);
 
+/* Dump files (dump.c:24-191).  The scalars of the dump header that the step
+   itself does not know (the coordinate plugin's parameters). */
+typedef struct harm_dump_header {
+  double startx1, startx2;  /* startx[1], startx[2] */
+  double a;                 /* black-hole spin */
+  double R0, Rin, Rout, hslope;
+  int defcoord;
+} harm_dump_header;
+
+/* Writes the reference's text dump file (dump(): dump_header + dump_content
+   through dump_gen with TEXTOUTPUT, dump.c:24-191, 641-960) of the device
+   state to `path`: one header line (t, N1, N2, startx, dx, realnstep, gam,
+   a, R0, Rin, Rout, hslope, dt, defcoord) and one line per active zone, x1
+   fastest, of 56 "%21.15g " columns: i, j, X1, X2, r, th, p (8), divb, u^mu,
+   u_mu, b^mu, b_mu, vmin/vmax in x1 and x2, sqrt(-g), J^mu, J_mu, F^{mu nu},
+   F_{mu nu}.  coords [n1m][n2m][4] holds X1, X2, r, th at zone centres (the
+   coordinate plugin's coord()/bl_coord()).  Needs a context created with
+   currents = 1 (the current columns).  Returns HARM_EFAIL if a wavespeed
+   evaluation failed (the reference's dump aborts there). */
+int harm_write_dump(harm_ctx* ctx, const char* path, const harm_dump_header* hdr, const double* coords);
+
 /* Diagnostics: runs one step outside the graph with a CUDA event after
    every kernel and returns, per kernel class (harm_kernel_name(k), k <
    HARM_NKERNELS), the summed device time in ms and the launch count. */

@@ -11,6 +11,8 @@
 #ifndef HARM_SETUP_H
 #define HARM_SETUP_H
 
+#include "harm_b200.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -48,6 +50,11 @@ int harm_torus_geometry(const harm_torus_params* p, double* gcov, double* gcon, 
    on the device, after harm_set_prims()). */
 int harm_torus_init(const harm_torus_params* p, const double* gcov, const double* gcon, const double* gdet,
                     double* prims);
+
+/* The coordinate columns of the torus grid for harm_write_dump(): the dump
+   header's plugin scalars (defcoord 0) and X1, X2, r, th at every zone
+   centre, [n1m][n2m][4] (coord.c:920-938, bl_coord coord.c:334-453). */
+int harm_torus_dump_coords(const harm_torus_params* p, harm_dump_header* hdr, double* coords);
 
 #ifdef __cplusplus
 }

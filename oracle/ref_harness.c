@@ -21,6 +21,7 @@
 #include "step_ch.h"
 #include <stdint.h>
 #include <string.h>
+#include <sys/stat.h>
 #include <unistd.h>
 
 /* ------------------------------------------------------------------ */
@@ -195,6 +196,39 @@ void hr_get_fluxes(double *f1, double *f2)
 {
   memcpy(f1, &a_F1[0][0][0], sizeof(a_F1));
   memcpy(f2, &a_F2[0][0][0], sizeof(a_F2));
+}
+
+/* the reference's own text dump file <workdir>/dumps/dump%04ld
+   (dump.c:24-46) of the current state */
+extern int hr_orig_dump(long dump_cnt);
+int hr_dump(const char *workdir, long cnt)
+{
+  char cwd[4096];
+  int rc;
+  if (!getcwd(cwd, sizeof(cwd))) return -1;
+  if (chdir(workdir) != 0) return -2;
+  mkdir("dumps", 0755);
+  rc = hr_orig_dump(cnt);
+  if (chdir(cwd) != 0) return -3;
+  return rc;
+}
+int hr_get_defcoord(void) { return defcoord; }
+
+/* X1, X2, r, th at zone centres (coord() and bl_coord()), [N1M][N2M][4] */
+void hr_get_coords(double *out)
+{
+  int i, j;
+  FTYPE X[NDIM], r, th;
+  for (i = -N1BND; i < N1 + N1BND; i++)
+    for (j = -N2BND; j < N2 + N2BND; j++) {
+      double *o = out + ((size_t)(i + N1BND) * N2M + (j + N2BND)) * 4;
+      coord(i, j, CENT, X);
+      bl_coord(X, &r, &th);
+      o[0] = X[1];
+      o[1] = X[2];
+      o[2] = r;
+      o[3] = th;
+    }
 }
 
 /* diagnostic currents (phys.c:1124-1455): jcon [N1M][N2M][4], fcon

@@ -146,7 +146,7 @@ def ref_lib_path(n1, n2, problem="torus"):
     return p if os.path.exists(p) else None
 
 
-def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
+def _ref_worker(libpath, lim, flux, cour, nsteps, outpath, dump=False):
     """Runs in a child process: reference init + nsteps steps, pickled to outpath."""
     import pickle
     lib = ctypes.CDLL(libpath)
@@ -202,13 +202,27 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath):
     f1 = np.zeros((m1, m2, 8))
     f2 = np.zeros((m1, m2, 8))
     lib.hr_get_fluxes(V(f1), V(f2))
+    if dump:
+        # the reference's own dump file of the final state (cwd is the work dir)
+        os.dup2(devnull, 2)
+        lib.hr_dump.argtypes = [ctypes.c_char_p, ctypes.c_long]
+        rcd = lib.hr_dump(work.encode(), 0)
+        os.dup2(saved, 2)
+        if rcd != 0:
+            raise RuntimeError("reference dump failed")
+        with open(os.path.join(work, "dumps", "dump0000"), "rb") as fd:
+            extra["dump"] = fd.read()
+        co = np.zeros((m1, m2, 4))
+        lib.hr_get_coords(V(co))
+        extra["coords"] = co
+        extra["defcoord"] = lib.hr_get_defcoord()
     with open(outpath, "wb") as f:
         pickle.dump(dict(n1=n1, n2=n2, scalars=scal0, geom=geom, prims=ps, pflag=pfs, times=ts, horizon=hz, F1=f1, F2=f2,
                          currents=cur,
                          ncyclebreak=lib.hr_get_ncyclebreak(), **extra), f, protocol=4)
 
 
-def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800):
+def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800, dump=False):
     """Runs the compiled reference (init + nsteps steps) in a fresh child
     process (its init() can run once per process) and returns its arrays."""
     import pickle
@@ -218,8 +232,8 @@ def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=
         return None
     fd, out = tempfile.mkstemp(suffix=".pkl", prefix="harmref_")
     os.close(fd)
-    code = ("import sys; sys.path.insert(0, %r); import harmtest; harmtest._ref_worker(%r, %d, %d, %r, %d, %r)"
-            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, float(cour), nsteps, out))
+    code = ("import sys; sys.path.insert(0, %r); import harmtest; harmtest._ref_worker(%r, %d, %d, %r, %d, %r, %r)"
+            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, float(cour), nsteps, out, bool(dump)))
     try:
         r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:

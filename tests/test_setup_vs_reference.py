@@ -19,3 +19,14 @@ def test_setup_matches_reference(harm, n):
     p = harm.torus_init(harm.torus_params(n, n), g)
     I = ht.interior
     assert np.array_equal(I(p)[..., :7], I(r["prims"][0])[..., :7])
+
+
+def test_torus_dump_coords_match_reference(harm):
+    r = ht.ref_run(32, 32, lim=3, flux=1, nsteps=0, dump=True)
+    if r is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    hdr, co = harm.torus_dump_coords(harm.torus_params(32, 32))
+    assert np.array_equal(co, r["coords"])
+    s = r["scalars"]
+    ref = dict(startx1=s[8], startx2=s[9], a=s[2], R0=s[7], Rin=s[4], Rout=s[5], hslope=s[6], defcoord=r["defcoord"])
+    assert all(hdr[k] == ref[k] for k in ref), (hdr, ref)
