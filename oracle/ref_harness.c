@@ -214,6 +214,20 @@ int hr_dump(const char *workdir, long cnt)
 }
 int hr_get_defcoord(void) { return defcoord; }
 
+/* the reference's own restart file <workdir>/dumps/rdump-%01ld
+   (restart_write, restart.c:182-222) of the current state */
+int hr_restart_write(const char *workdir, long cnt)
+{
+  char cwd[4096];
+  int rc;
+  if (!getcwd(cwd, sizeof(cwd))) return -1;
+  if (chdir(workdir) != 0) return -2;
+  mkdir("dumps", 0755);
+  rc = restart_write(cnt);
+  if (chdir(cwd) != 0) return -3;
+  return rc;
+}
+
 /* X1, X2, r, th at zone centres (coord() and bl_coord()), [N1M][N2M][4] */
 void hr_get_coords(double *out)
 {

@@ -212,6 +212,14 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath, dump=False):
             raise RuntimeError("reference dump failed")
         with open(os.path.join(work, "dumps", "dump0000"), "rb") as fd:
             extra["dump"] = fd.read()
+        lib.hr_restart_write.argtypes = [ctypes.c_char_p, ctypes.c_long]
+        os.dup2(devnull, 2)
+        rcr = lib.hr_restart_write(work.encode(), 0)
+        os.dup2(saved, 2)
+        if rcr != 0:
+            raise RuntimeError("reference restart_write failed")
+        with open(os.path.join(work, "dumps", "rdump-0"), "rb") as fd:
+            extra["rdump"] = fd.read()
         co = np.zeros((m1, m2, 4))
         lib.hr_get_coords(V(co))
         extra["coords"] = co

@@ -55,3 +55,53 @@ def test_dump_file_matches_reference_bytes(harm, problem, n1, n2, lim, flux, nst
     mine = _dump_bytes(h, _header(r), r["coords"])
     assert mine == r["dump"], _first_difference(mine, r["dump"])
     h.close()
+
+
+def test_restart_on_device_from_reference_rdump(harm):
+    """A reference restart file continued on the device: the state read from
+    it, uploaded and bounded, steps exactly as the oracle steps it; the
+    device state written back out reads in again unchanged (to the file's
+    15 digits)."""
+    from harm_ramt_b200 import restart as R
+    n, lim, flux, nsteps = 32, 4, 1, 20
+    r = ht.ref_run(n, n, lim=lim, flux=flux, nsteps=5, dump=True)
+    if r is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    d = tempfile.mkdtemp(prefix="harm_rdump_")
+    src = os.path.join(d, "rdump-0")
+    with open(src, "wb") as f:
+        f.write(r["rdump"])
+    rd = R.read_rdump(src)
+    p0 = np.zeros((n + 6, n + 6, 8))
+    p0[3:-3, 3:-3] = rd["prims"]
+    cfg = ht.ref_config(r)
+    g = r["geom"]
+    h = harm.HarmGPU(n, n, cfg.pop("dx1"), cfg.pop("dx2"), lim=lim, fluxmethod=flux, **cfg)
+    h.upload_geometry(g["gcov"], g["gcon"], g["gdet"], g["conn"], g["floors"])
+    h.set_prims(p0)
+    h.bound_prims()
+    hd = rd["header"]
+    h.set_time(hd["t"], hd["dt"], hd["realnstep"])
+    o = ht.Oracle(n, n, g, lim=lim, fluxmethod=flux, **ht.ref_config(r))
+    po = o.bound(p0)
+    fo = np.zeros(po.shape[:2] + (5,), dtype=np.int32)
+    pg, _ = h.get_prims()
+    assert np.array_equal(pg, po)
+    t, dt = hd["t"], hd["dt"]
+    for _ in range(nsteps):
+        rc, t, dt = o.step(po, fo, t, dt)
+        assert rc == 0
+    h.step_ch(nsteps)
+    st = h.sync()
+    pg, fg = h.get_prims()
+    assert np.array_equal(pg, po) and (st["t"], st["dt"]) == (t, dt)
+    assert st["realnstep"] == hd["realnstep"] + nsteps
+    out = os.path.join(d, "rdump-1")
+    R.write_rdump(out, R.rdump_header_from_context(h, hd), pg, rd["accounting"], rd["rescaletype"], rd["lumvsr"])
+    back = R.read_rdump(out)
+    assert np.array_equal(back["prims"], np.vectorize(lambda x: float("%.15g" % x))(pg[3:-3, 3:-3]))
+    assert back["header"]["realnstep"] == st["realnstep"]
+    h.close()
+    for fn in (src, out):
+        os.unlink(fn)
+    os.rmdir(d)
