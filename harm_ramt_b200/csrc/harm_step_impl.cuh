@@ -116,8 +116,10 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // states once: the x1 neighbour's right state arrives by warp shuffle and
 // the x2 neighbour's through shared memory (the first lane/row recomputes).
 constexpr int FLUX_BY = 4;
+// FP64: at most 128 registers (4 blocks per SM); the register-light FP32
+// faces of the mixed form are left unconstrained
 template <typename T, bool PARA, bool FFDE>
-__global__ void __launch_bounds__(32 * FLUX_BY) k_flux(StepArgs a, const double* __restrict__ pb)
+__global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 4 : 1) k_flux(StepArgs a, const double* __restrict__ pb)
 {
   __shared__ double sh[2][32];
   __shared__ T shr[NPR][FLUX_BY][32];
