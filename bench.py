@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--accuracy-t", type=float, default=100.0,
                     help="time (GM/c^3) to which FP64 and mixed runs go from init for the L1 comparison")
+    ap.add_argument("--ensemble", type=int, default=64, help="tori in the batched-ensemble leg (0: skip it)")
+    ap.add_argument("--ensemble-steps", type=int, default=200)
+    ap.add_argument("--ensemble-steps-per-launch", type=int, default=10)
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
@@ -310,6 +313,9 @@ def b200_arm(a):
     mixed = None
     if not a.no_mixed:
         mixed = mixed_precision_leg(a, hb, stream, lim, flux, value, barrier, dist)
+    ens = None
+    if a.ensemble > 0:
+        ens = ensemble_leg(a, hb, stream, lim, flux, barrier, dist)
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -334,12 +340,74 @@ def b200_arm(a):
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
+                "ensemble": ens,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def ensemble_leg(a, hb, stream, lim, flux, barrier, dist):
+    """The batched form: a.ensemble tori of uneven size and parameters
+    (harm_ramt_b200.ensemble.sample_tori), tile shapes autotuned per torus,
+    a.ensemble_steps steps of all of them (1) as one CUDA graph launch per
+    a.ensemble_steps_per_launch steps holding every torus as a branch, and
+    (2) torus after torus, each with its own per-step graph launches, from
+    the same initial states.  Aggregate zone-cycles/s of both, FP64 and
+    mixed; max over ranks."""
+    import torch
+    from harm_ramt_b200 import autotune
+    from harm_ramt_b200 import ensemble as ens
+    specs = ens.sample_tori(a.ensemble, seed=7)
+    zones = sum(s["n1"] * s["n2"] for s in specs)
+    K, S = a.ensemble_steps, a.ensemble_steps_per_launch
+    K -= K % S
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    out = {"tori": a.ensemble, "zones_per_step": zones, "steps": K, "steps_per_launch": S,
+           "sizes": "N1, N2 uniform in {64, 96, ..., 384}; a ~ U[0, 0.99]; beta log-uniform [10, 1000]; "
+                    "rmax ~ U[10, 16]; seed 7"}
+
+    def timed(fn):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+
+    for name, prec in (("fp64", hb.PREC_FP64), ("mixed", hb.PREC_MIXED)):
+        members = ens.build(hb, specs, lim=lim, fluxmethod=flux, precision=prec, stream=stream.cuda_stream)
+        tiles = {}
+        for (h, p0), s in zip(members, specs):
+            up, sm, _ = autotune.tune(h, reps=2, key=(s["n1"], s["n2"], prec, lim, flux))
+            tiles[f"{up[0]}x{up[1]}/{sm[0]}x{sm[1]}"] = tiles.get(f"{up[0]}x{up[1]}/{sm[0]}x{sm[1]}", 0) + 1
+            ens.reset(h, p0)
+        hs = [h for h, _ in members]
+        for h in hs:  # capture each member's own step graph outside the timed region
+            h.step_ch(1)
+        for (h, p0) in members:
+            ens.reset(h, p0)
+        ms_seq = timed(lambda: [h.step_ch(K) for h in hs])
+        failed_seq = [k for k, h in enumerate(hs) if h.sync(raise_on_fail=False)["fail_code"]]
+        for (h, p0) in members:
+            ens.reset(h, p0)
+        e = hb.Ensemble(hs, steps_per_launch=S, stream=stream.cuda_stream)
+        ms_ens = timed(lambda: e.step(K))
+        st = e.sync(raise_on_fail=False)
+        failed = [k for k, s in enumerate(st) if s["fail_code"]]
+        e.close()
+        for h in hs:
+            h.close()
+        v_ens = aggregate_rate(world, zones, ms_ens * 1e-3 / K)
+        v_seq = aggregate_rate(world, zones, ms_seq * 1e-3 / K)
+        out[name] = {"graph_batched": v_ens, "sequential_per_torus": v_seq, "speedup": v_ens / v_seq,
+                     "ms_per_step_batched": ms_ens / K, "ms_per_step_sequential": ms_seq / K,
+                     "tiles_chosen": tiles, "failed_members": failed, "failed_members_sequential": failed_seq}
+    return out
 
 
 # diagnostic times of the accuracy curve (GM/c^3); the last one is --accuracy-t

@@ -24,7 +24,7 @@ import numpy as np
 
 __all__ = ["HarmGPU", "HarmError", "torus_params", "torus_geometry", "torus_init", "load_library", "LIB_PATH",
            "LIM_MC", "LIM_PARA", "FLUX_LAXF", "FLUX_HLL", "PREC_FP64", "PREC_MIXED", "EOM_GRMHD", "EOM_FFDE",
-           "BC_TORUS", "BC_STAR", "NG", "NPR", "pinned_empty", "torus_context", "torus_dump_coords"]
+           "BC_TORUS", "BC_STAR", "NG", "NPR", "pinned_empty", "torus_context", "torus_dump_coords", "Ensemble"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libharm_b200.so")
 NG = 3
@@ -66,6 +66,11 @@ class _DumpHeader(ctypes.Structure):
                 ("hslope", ctypes.c_double), ("defcoord", ctypes.c_int)]
 
 
+class _Tiles(ctypes.Structure):
+    _fields_ = [("update_x", ctypes.c_int), ("update_y", ctypes.c_int), ("small_x", ctypes.c_int),
+                ("small_y", ctypes.c_int)]
+
+
 class _Status(ctypes.Structure):
     _fields_ = [("fail_code", ctypes.c_int), ("fail_i", ctypes.c_int), ("fail_j", ctypes.c_int),
                 ("fixups", ctypes.c_int), ("realnstep", ctypes.c_longlong), ("t", ctypes.c_double),
@@ -87,7 +92,8 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_set_time", "harm_step", "harm_sync", "harm_get_fluxes", "harm_destroy", "harm_error_string",
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
            "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
-           "harm_torus_dump_coords"]
+           "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
+           "harm_ensemble_sync", "harm_ensemble_destroy"]
 
 
 def load_library(path=None):
@@ -129,6 +135,13 @@ def load_library(path=None):
     lib.harm_get_horizon.argtypes = [vp, dp]
     lib.harm_get_currents.argtypes = [vp, dp, dp, dp]
     lib.harm_write_dump.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(_DumpHeader), dp]
+    lib.harm_set_tiles.argtypes = [vp, ctypes.POINTER(_Tiles)]
+    lib.harm_get_tiles.argtypes = [vp, ctypes.POINTER(_Tiles)]
+    lib.harm_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, vp, ctypes.POINTER(vp)]
+    lib.harm_ensemble_step.argtypes = [vp, ctypes.c_int]
+    lib.harm_ensemble_sync.argtypes = [vp, ctypes.POINTER(_Status)]
+    lib.harm_ensemble_destroy.argtypes = [vp]
+    lib.harm_ensemble_destroy.restype = None
     lib.harm_torus_dump_coords.argtypes = [ctypes.POINTER(_TorusParams), ctypes.POINTER(_DumpHeader), dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
@@ -324,6 +337,17 @@ class HarmGPU:
         assert co.shape == (self.n1m, self.n2m, 4)
         _check(self.lib.harm_write_dump(self._h, os.fsencode(path), ctypes.byref(h), _dp(co)), "harm_write_dump")
 
+    def set_tiles(self, update=(32, 4), small=(32, 4)):
+        """Block shapes of k_update (<= 128 threads) and of the small
+        stencil kernels (<= 1024 threads)."""
+        t = _Tiles(int(update[0]), int(update[1]), int(small[0]), int(small[1]))
+        _check(self.lib.harm_set_tiles(self._h, ctypes.byref(t)), "harm_set_tiles")
+
+    def get_tiles(self):
+        t = _Tiles()
+        _check(self.lib.harm_get_tiles(self._h, ctypes.byref(t)), "harm_get_tiles")
+        return (t.update_x, t.update_y), (t.small_x, t.small_y)
+
     def get_fluxes(self):
         f1 = np.zeros((self.n1m, self.n2m, NPR))
         f2 = np.zeros((self.n1m, self.n2m, NPR))
@@ -338,6 +362,45 @@ def pinned_empty(shape, dtype=np.float64):
     t = torch.empty(tuple(shape), dtype={np.float64: torch.float64, np.int32: torch.int32}[np.dtype(dtype).type],
                     pin_memory=True)
     return t.numpy()
+
+
+class Ensemble:
+    """Several HarmGPU contexts advanced together: each ensemble step is one
+    CUDA graph launch holding every member's step as an independent branch
+    (harm_ensemble_create); steps_per_launch > 1 unrolls steps into it."""
+
+    def __init__(self, members, steps_per_launch=1, stream=None):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        h = ctypes.c_void_p()
+        _check(self.lib.harm_ensemble_create(arr, len(self.members), int(steps_per_launch),
+                                             ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_ensemble_create")
+        self._h = h
+        self.steps_per_launch = int(steps_per_launch)
+
+    def step(self, nsteps):
+        _check(self.lib.harm_ensemble_step(self._h, int(nsteps)), "harm_ensemble_step")
+
+    def sync(self, raise_on_fail=True):
+        st = (_Status * len(self.members))()
+        rc = self.lib.harm_ensemble_sync(self._h, st)
+        out = [dict(fail_code=s.fail_code, fail_i=s.fail_i, fail_j=s.fail_j, fixups=s.fixups, realnstep=s.realnstep,
+                    t=s.t, dt=s.dt, newton_iters=s.newton_iters) for s in st]
+        if rc == 6 and raise_on_fail:
+            bad = [k for k, s in enumerate(out) if s["fail_code"]]
+            raise HarmError(rc, f"ensemble members {bad} failed")
+        if rc not in (0, 6):
+            raise HarmError(rc, "harm_ensemble_sync")
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.harm_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def torus_dump_coords(params):

@@ -61,6 +61,8 @@ struct harm_ctx {
   cudaGraph_t graph;
   cudaGraphExec_t gexec;
   bool have_graph;
+  dim3 tile_update;  // k_update block (at most 128 threads)
+  dim3 tile_small;   // block of the stencil/fixup/boundary kernels
   StepArgs args() const
   {
     StepArgs a;
@@ -143,7 +145,9 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
   Timer& T = tm ? *tm : dummy;
   const StepArgs a = c->args();
   const int n1 = c->cfg.n1, n2 = c->cfg.n2;
-  const dim3 b(32, 4);
+  const dim3 fb(32, FLUX_BY);     // k_flux's shape is fixed by its warp/shared-memory state sharing
+  const dim3 b = c->tile_small;   // the other stencil kernels
+  const dim3 ub = c->tile_update;
   cudaStream_t s = c->stream;
   k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
   T.mark(s, KC_BSQ);
@@ -155,11 +159,11 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     const int mixed = c->cfg.precision == HARM_PREC_MIXED;
     const int ffde = c->cfg.eom == HARM_EOM_FFDE;
     const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, grid2(n1 + 2, n2 + 2, b), b, s, a, pb);
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, grid2(n1 + 2, n2 + 2, fb), fb, s, a, pb);
     T.mark(s, KC_FLUX);
     launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
-    launch_update(mixed, ffde, grid2(n1, n2, b), b, s, a, pi, pb, pf, c2);
+    launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE);
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
@@ -249,8 +253,10 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   c->gr.plane = (long long)c->gr.pitch * c->gr.rows;
   const size_t pd = (size_t)c->gr.plane * sizeof(double);
   const dim3 b(32, 4);
-  dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, b);
+  dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, dim3(32, FLUX_BY));
   c->nblocks_flux = gf.x * gf.y;
+  c->tile_update = dim3(32, 4);
+  c->tile_small = dim3(32, 4);
   bool ok = true;
   ok &= cudaMalloc(&c->d_p, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_pk0, NPR * pd) == cudaSuccess;
@@ -606,6 +612,145 @@ int harm_write_dump(harm_ctx* c, const char* path, const harm_dump_header* hdr, 
   return ok ? HARM_OK : HARM_EINVAL;
 }
 
+static void drop_graph(harm_ctx* c)
+{
+  if (c->have_graph) {
+    cudaGraphExecDestroy(c->gexec);
+    cudaGraphDestroy(c->graph);
+    c->have_graph = false;
+  }
+}
+
+int harm_set_tiles(harm_ctx* c, const harm_tiles* t)
+{
+  if (!c || !t) return HARM_EINVAL;
+  const long long nu = (long long)t->update_x * t->update_y, ns = (long long)t->small_x * t->small_y;
+  if (t->update_x < 1 || t->update_y < 1 || nu > 128 || t->small_x < 1 || t->small_y < 1 || ns > 1024)
+    return HARM_EINVAL;
+  CK(cudaStreamSynchronize(c->stream));
+  c->tile_update = dim3(t->update_x, t->update_y);
+  c->tile_small = dim3(t->small_x, t->small_y);
+  drop_graph(c);
+  return HARM_OK;
+}
+
+int harm_get_tiles(harm_ctx* c, harm_tiles* t)
+{
+  if (!c || !t) return HARM_EINVAL;
+  t->update_x = c->tile_update.x;
+  t->update_y = c->tile_update.y;
+  t->small_x = c->tile_small.x;
+  t->small_y = c->tile_small.y;
+  return HARM_OK;
+}
+
+// ---------------------------------------------------------------- ensembles
+struct harm_ensemble {
+  std::vector<harm_ctx*> m;
+  int per_launch;
+  cudaStream_t stream;
+  bool own_stream;
+  cudaGraph_t graph;
+  cudaGraphExec_t gexec;
+};
+
+void harm_ensemble_destroy(harm_ensemble* e)
+{
+  if (!e) return;
+  cudaStreamSynchronize(e->stream);
+  if (e->gexec) cudaGraphExecDestroy(e->gexec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->own_stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int harm_ensemble_create(harm_ctx* const* members, int n, int per_launch, void* stream, harm_ensemble** out)
+{
+  if (!members || n < 1 || per_launch < 1 || !out) return HARM_EINVAL;
+  for (int k = 0; k < n; k++)
+    if (!members[k] || !members[k]->geo_ok) return HARM_EINVAL;
+  harm_ensemble* e = new harm_ensemble();
+  e->m.assign(members, members + n);
+  e->per_launch = per_launch;
+  e->stream = (cudaStream_t)stream;
+  e->own_stream = false;
+  e->graph = nullptr;
+  e->gexec = nullptr;
+  if (!e->stream) {
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete e;
+      return HARM_ECUDA;
+    }
+    e->own_stream = true;
+  }
+  // members' pending work (uploads, set-up) completes before the first launch
+  for (int k = 0; k < n; k++)
+    if (cudaStreamSynchronize(members[k]->stream) != cudaSuccess) {
+      harm_ensemble_destroy(e);
+      return HARM_ECUDA;
+    }
+  // capture: fork from the ensemble stream into one branch stream per
+  // member, each branch the member's step sequence, joined at the end
+  std::vector<cudaStream_t> br(n, nullptr);
+  std::vector<cudaEvent_t> ev(n + 1, nullptr);
+  int rc = HARM_OK;
+  bool ok = true;
+  for (int k = 0; k < n && ok; k++) ok = cudaStreamCreateWithFlags(&br[k], cudaStreamNonBlocking) == cudaSuccess;
+  for (int k = 0; k <= n && ok; k++) ok = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) == cudaSuccess;
+  if (ok) ok = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    bool cap_ok = cudaEventRecord(ev[n], e->stream) == cudaSuccess;
+    for (int k = 0; k < n && cap_ok; k++) {
+      cap_ok = cudaStreamWaitEvent(br[k], ev[n], 0) == cudaSuccess;
+      harm_ctx tmp = *e->m[k];
+      tmp.stream = br[k];
+      for (int sidx = 0; sidx < per_launch && cap_ok; sidx++) cap_ok = enqueue_step(&tmp) == HARM_OK;
+      if (cap_ok) cap_ok = cudaEventRecord(ev[k], br[k]) == cudaSuccess;
+      if (cap_ok) cap_ok = cudaStreamWaitEvent(e->stream, ev[k], 0) == cudaSuccess;
+    }
+    cudaGraph_t g = nullptr;
+    const bool end_ok = cudaStreamEndCapture(e->stream, &g) == cudaSuccess;
+    ok = cap_ok && end_ok;
+    if (ok) ok = cudaGraphInstantiate(&e->gexec, g, 0) == cudaSuccess;
+    e->graph = g;
+  }
+  for (int k = 0; k < n; k++)
+    if (br[k]) cudaStreamDestroy(br[k]);
+  for (int k = 0; k <= n; k++)
+    if (ev[k]) cudaEventDestroy(ev[k]);
+  if (!ok) {
+    fprintf(stderr, "harm_b200: harm_ensemble_create: graph capture failed (%s)\n",
+            cudaGetErrorString(cudaGetLastError()));
+    harm_ensemble_destroy(e);
+    return HARM_ECUDA;
+  }
+  (void)rc;
+  *out = e;
+  return HARM_OK;
+}
+
+int harm_ensemble_step(harm_ensemble* e, int nsteps)
+{
+  if (!e || nsteps < 0 || nsteps % e->per_launch) return HARM_EINVAL;
+  for (int k = 0; k < nsteps / e->per_launch; k++) CK(cudaGraphLaunch(e->gexec, e->stream));
+  return HARM_OK;
+}
+
+int harm_ensemble_sync(harm_ensemble* e, harm_status* st)
+{
+  if (!e) return HARM_EINVAL;
+  CK(cudaStreamSynchronize(e->stream));
+  int worst = HARM_OK;
+  for (size_t k = 0; k < e->m.size(); k++) {
+    harm_status s;
+    const int rc = harm_sync(e->m[k], &s);
+    if (st) st[k] = s;
+    if (rc == HARM_EFAIL) worst = HARM_EFAIL;
+    else if (rc != HARM_OK) return rc;
+  }
+  return worst;
+}
+
 int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)
 {
   if (!c || !ms || !launches || nclasses < KC_COUNT) return HARM_EINVAL;
@@ -732,8 +877,10 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.gr.rows = c.n2m;
   c.gr.plane = (long long)c.gr.pitch * c.gr.rows;
   const dim3 b(32, 4);
-  const dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, b);
+  const dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, dim3(32, FLUX_BY));
   c.nblocks_flux = gf.x * gf.y;
+  c.tile_update = dim3(32, 4);
+  c.tile_small = dim3(32, 4);
   if (c.gr.plane > NOALLOC_MAX_PLANE || c.nblocks_flux > NOALLOC_MAX_BLOCKS) {
     fprintf(stderr,
             "harm_step_noalloc: a %d x %d grid needs %lld doubles per plane; the static scratch holds %lld "

@@ -114,6 +114,9 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
 
+// k_flux blocks: 32 zones along x1 (one warp) x FLUX_BY rows
+constexpr int FLUX_BY = 4;
+
 // plane offsets of the currents block
 constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 21, CUR_NPLANES = 25;
 

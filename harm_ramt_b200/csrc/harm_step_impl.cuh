@@ -115,7 +115,6 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
 // states once: the x1 neighbour's right state arrives by warp shuffle and
 // the x2 neighbour's through shared memory (the first lane/row recomputes).
-constexpr int FLUX_BY = 4;
 // FP64: at most 128 registers (4 blocks per SM); the register-light FP32
 // faces of the mixed form are left unconstrained
 template <typename T, bool PARA, bool FFDE>

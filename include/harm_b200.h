@@ -187,6 +187,35 @@ typedef struct harm_dump_header {
    evaluation failed (the reference's dump aborts there). */
 int harm_write_dump(harm_ctx* ctx, const char* path, const harm_dump_header* hdr, const double* coords);
 
+/* Thread-block shapes of the step's kernels (k_flux's is fixed: one warp
+   along x1 by 4 rows).  update: k_update, at most 128 threads; small: the
+   flag, EMF, boundary, check-solution and repair kernels, at most 1024
+   threads.  Default 32 x 4 for both.  Changing them re-captures the step. */
+typedef struct harm_tiles {
+  int update_x, update_y;
+  int small_x, small_y;
+} harm_tiles;
+int harm_set_tiles(harm_ctx* ctx, const harm_tiles* tiles);
+int harm_get_tiles(harm_ctx* ctx, harm_tiles* tiles);
+
+/* Ensembles: several contexts (independent grids of any sizes, e.g. tori of
+   different resolutions and parameters) advanced together.  One step of
+   the ensemble is one CUDA graph launch holding every member's step as an
+   independent branch, so small grids run side by side on the GPU instead of
+   one after another; steps_per_launch > 1 unrolls that many steps into the
+   graph.  Members keep their own state and are read with the usual calls
+   after harm_ensemble_sync(); a member must not be stepped on its own
+   while it belongs to an ensemble. */
+typedef struct harm_ensemble harm_ensemble;
+int harm_ensemble_create(harm_ctx* const* members, int n, int steps_per_launch, void* stream, harm_ensemble** out);
+/* Enqueues nsteps steps of every member (nsteps a multiple of
+   steps_per_launch) on the ensemble's stream. */
+int harm_ensemble_step(harm_ensemble* e, int nsteps);
+/* Waits for the ensemble's stream; st (may be NULL) receives n statuses.
+   Returns HARM_EFAIL if any member hit a fatal check. */
+int harm_ensemble_sync(harm_ensemble* e, harm_status* st);
+void harm_ensemble_destroy(harm_ensemble* e);
+
 /* Diagnostics: runs one step outside the graph with a CUDA event after
    every kernel and returns, per kernel class (harm_kernel_name(k), k <
    HARM_NKERNELS), the summed device time in ms and the launch count. */
