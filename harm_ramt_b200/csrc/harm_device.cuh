@@ -25,6 +25,10 @@ enum { FAIL_VCHAR_DISCR = 3, FAIL_COEFF_NEG = 4, FAIL_COEFF_SUP = 5, FAIL_UTCALC
 // reference aborts the step through MYFUN without a FAIL_* number
 constexpr int FAIL_FFDE_SPACELIKE = 20;
 
+// host-and-device inline: the per-zone physics also compiles for the host,
+// where the adjoint's building blocks are checked against finite differences
+#define HD_INLINE __host__ __device__ __forceinline__
+
 constexpr double DBL_EPS_REF = 2.2204460492503131e-16;  // global.h:710
 
 __host__ __device__ constexpr int sym(int a, int b)
@@ -42,11 +46,11 @@ struct Geo {
 };
 
 template <typename T>
-__device__ __forceinline__ T rmax(T a, T b) { return (a > b) ? a : b; }  // phys.c:1580
+HD_INLINE T rmax(T a, T b) { return (a > b) ? a : b; }  // phys.c:1580
 template <typename T>
-__device__ __forceinline__ T rmin(T a, T b) { return (a > b) ? b : a; }  // phys.c:1587
+HD_INLINE T rmin(T a, T b) { return (a > b) ? b : a; }  // phys.c:1587
 template <typename T>
-__device__ __forceinline__ T rsign(T a) { return (a > T(0.0)) ? T(1.0) : ((a < T(0.0)) ? T(-1.0) : T(0.0)); }
+HD_INLINE T rsign(T a) { return (a > T(0.0)) ? T(1.0) : ((a < T(0.0)) ? T(-1.0) : T(0.0)); }
 
 template <typename T>
 struct State {
@@ -55,7 +59,7 @@ struct State {
 
 // gamma_calc, phys.c:848-877
 template <typename T>
-__device__ __forceinline__ T gamma_of(const T* pr, const Geo<T>& g)
+HD_INLINE T gamma_of(const T* pr, const Geo<T>& g)
 {
   const T* c = g.gcov;
   T qsq = c[4] * pr[U1] * pr[U1] + c[7] * pr[U2] * pr[U2] + c[9] * pr[U3] * pr[U3] +
@@ -65,7 +69,7 @@ __device__ __forceinline__ T gamma_of(const T* pr, const Geo<T>& g)
 
 // ucon_calc_rel4vel, phys.c:830-845
 template <typename T>
-__device__ __forceinline__ void ucon_of(const T* pr, const Geo<T>& g, T* ucon)
+HD_INLINE void ucon_of(const T* pr, const Geo<T>& g, T* ucon)
 {
   T alpha = T(1.) / sqrt(-g.gcon[0]);
   T beta1 = g.gcon[1] * alpha * alpha;
@@ -80,7 +84,7 @@ __device__ __forceinline__ void ucon_of(const T* pr, const Geo<T>& g, T* ucon)
 
 // lower, phys.c:633
 template <typename T>
-__device__ __forceinline__ void lower_v(const T* v, const T* c, T* w)
+HD_INLINE void lower_v(const T* v, const T* c, T* w)
 {
   w[0] = c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3];
   w[1] = c[1] * v[0] + c[4] * v[1] + c[5] * v[2] + c[6] * v[3];
@@ -89,11 +93,11 @@ __device__ __forceinline__ void lower_v(const T* v, const T* c, T* w)
 }
 
 template <typename T>
-__device__ __forceinline__ T dot4(const T* a, const T* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3]; }
+HD_INLINE T dot4(const T* a, const T* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3]; }
 
 // get_state + bcon_calc, phys.c:716-727 and 285-294
 template <typename T>
-__device__ __forceinline__ void state_of(const T* pr, const Geo<T>& g, State<T>& q)
+HD_INLINE void state_of(const T* pr, const Geo<T>& g, State<T>& q)
 {
   ucon_of(pr, g, q.ucon);
   lower_v(q.ucon, g.gcov, q.ucov);
@@ -105,7 +109,7 @@ __device__ __forceinline__ void state_of(const T* pr, const Geo<T>& g, State<T>&
 
 // mhd_calc_0, phys.c:381-406 (row `dir` of T^mu_nu)
 template <typename T, bool FFDE>
-__device__ __forceinline__ void mhd_row(const T* pr, int dir, const State<T>& q, T gam, T* mhd)
+HD_INLINE void mhd_row(const T* pr, int dir, const State<T>& q, T gam, T* mhd)
 {
   T r, u, P, w;
   if (!FFDE) {
@@ -126,7 +130,7 @@ __device__ __forceinline__ void mhd_row(const T* pr, int dir, const State<T>& q,
 // primtoflux(UEVOLVE), phys.c:16-56, massflux_calc 59, dualfullfaraday_calc
 // (PRIMMAXWELL) 155-185, UtoU(UNOTHING->UEVOLVE) 219-265
 template <typename T, bool FFDE>
-__device__ __forceinline__ void flux_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T* F)
+HD_INLINE void flux_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T* F)
 {
   T fin[NPR];
   fin[RHO] = pr[RHO] * q.ucon[dir];
@@ -149,7 +153,7 @@ __device__ __forceinline__ void flux_of(const T* pr, const State<T>& q, int dir,
 // reduce to metric columns, so the dot products are the metric entries the
 // reference's zero-padded sums produce.  Returns a fail code.
 template <typename T>
-__device__ __forceinline__ int vchar_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T& vmax, T& vmin)
+HD_INLINE int vchar_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T& vmax, T& vmin)
 {
   // NUMEPSILON*100 of the reference's FTYPE (global.h:706-727): DBL_EPSILON
   // for FP64, FLT_EPSILON for the FP32 faces of the mixed form
@@ -211,7 +215,7 @@ __device__ __forceinline__ int vchar_of(const T* pr, const State<T>& q, int dir,
 
 // limit_gamma, fixup.c:1298-1354.  Returns a fail code.
 template <typename T>
-__device__ __forceinline__ int limit_gamma(T gammamax, T* pr, const Geo<T>& g)
+HD_INLINE int limit_gamma(T gammamax, T* pr, const Geo<T>& g)
 {
   if (gammamax <= T(1.0)) return 0;
   T gamma = gamma_of(pr, g);
@@ -228,9 +232,9 @@ __device__ __forceinline__ int limit_gamma(T gammamax, T* pr, const Geo<T>& g)
 
 // MC slope, interp.c:106-118 with MINMOD, interp.h:13-14
 template <typename T>
-__device__ __forceinline__ T minmod(T a, T b) { return (a * b <= T(0)) ? T(0.0) : ((fabs(a) < fabs(b)) ? a : b); }
+HD_INLINE T minmod(T a, T b) { return (a * b <= T(0)) ? T(0.0) : ((fabs(a) < fabs(b)) ? a : b); }
 template <typename T>
-__device__ __forceinline__ T mc_slope(T yl, T yc, T yr)
+HD_INLINE T mc_slope(T yl, T yc, T yr)
 {
   T Dqm = T(2.0) * (yc - yl);
   T Dqp = T(2.0) * (yr - yc);
@@ -240,7 +244,7 @@ __device__ __forceinline__ T mc_slope(T yl, T yc, T yr)
 
 // para4 with the MC sub-limiter, interp.c:444-538
 template <typename T>
-__device__ __forceinline__ void para4(T y0, T y1, T y2, T y3, T y4, T& lout, T& rout)
+HD_INLINE void para4(T y0, T y1, T y2, T y3, T y4, T& lout, T& rout)
 {
   T y[5] = {y0, y1, y2, y3, y4}, dq[5];
 #pragma unroll
@@ -275,7 +279,7 @@ __device__ __forceinline__ void para4(T y0, T y1, T y2, T y3, T y4, T& lout, T& 
 // Deterministic Newton cycle-break factor in [0,1): splitmix64 finaliser
 // (Steele, Lea & Flood 2014) of the iterate's bits and the iteration count.
 // Replaces rand()/RAND_MAX at utoprim_2d.c:669 (a serial global RNG stream).
-__device__ __forceinline__ uint64_t mix64(uint64_t z)
+HD_INLINE uint64_t mix64(uint64_t z)
 {
   z += 0x9E3779B97F4A7C15ULL;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -296,7 +300,7 @@ struct U2PCtx {
 };
 
 // utsq_calc, utoprim_2d.c:318-338
-__device__ __forceinline__ double utsq_calc(const U2PCtx& c, double W)
+HD_INLINE double utsq_calc(const U2PCtx& c, double W)
 {
   double Wsq = W * W, W4 = Wsq * Wsq;
   return (c.Bsq * c.QdotBsq + W * (2. * c.QdotBsq + c.Qtsq * W)) /
@@ -304,7 +308,7 @@ __device__ __forceinline__ double utsq_calc(const U2PCtx& c, double W)
 }
 
 // func_vsq Newton step, utoprim_2d.c:748-798
-__device__ __forceinline__ void func_vsq(const U2PCtx& c, double W, double vsq, double& dx0, double& dx1)
+HD_INLINE void func_vsq(const U2PCtx& c, double W, double vsq, double& dx0, double& dx1)
 {
   const double Bsq = c.Bsq, QdotBsq = c.QdotBsq, Qtsq = c.Qtsq, Qdotn = c.Qdotn, D = c.D, gam = c.gam;
   double Wsq = W * W;
@@ -369,7 +373,7 @@ __device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x
 
 // ucon_calc_3vel, phys.c:885-957: u^mu from v^i = u^i/u^t (packed gcov);
 // nonzero when the velocity is not time-like
-__device__ __forceinline__ int ucon_3vel(const double* v, const double* c, double* ucon)
+HD_INLINE int ucon_3vel(const double* v, const double* c, double* ucon)
 {
   const double discr = +c[0] + c[4] * v[1] * v[1] + c[7] * v[2] * v[2] + c[9] * v[3] * v[3] +
                        2. * (c[1] * v[1] + c[2] * v[2] + c[3] * v[3] + c[5] * v[1] * v[2] + c[6] * v[1] * v[3] +
@@ -389,7 +393,7 @@ __device__ __forceinline__ int ucon_3vel(const double* v, const double* c, doubl
 // 551-560), u^i through ucon_calc_3vel (vcon2pr's active branch,
 // transforms.c:372-377, stores u^i).  pr[RHO], pr[UU] keep the guess.
 // Returns 0 or FAIL_FFDE_SPACELIKE.
-__device__ __forceinline__ int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, double gammamax)
+HD_INLINE int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, double gammamax)
 {
   double U[NPR];
 #pragma unroll
@@ -435,7 +439,7 @@ __device__ __forceinline__ int utoprim_ffde(const double* Uin, const Geo<double>
 }
 
 // lower_g / raise_g of utoprim_2d.c:365-392: sums started from 0.
-__device__ __forceinline__ void lower_g(const double* v, const double* c, double* w)
+HD_INLINE void lower_g(const double* v, const double* c, double* w)
 {
 #pragma unroll
   for (int i = 0; i < 4; i++) {

@@ -1,0 +1,213 @@
+// Test harness (host code): each adjoint building block of
+// harm_ramt_b200/csrc/harm_adjoint.cuh against central finite differences
+// of its forward function, on given states and geometry.  Built with nvcc by
+// tests/test_adjoint_blocks.py; every check returns the relative error
+// |lambda . dF/dp v (finite difference) - pbar . v| / max(|.|, |.|).
+#include <math.h>
+#include <string.h>
+
+#include "../harm_ramt_b200/csrc/harm_adjoint.cuh"
+
+using namespace harm;
+
+namespace {
+
+Geo<double> geo_of(const double* gcov16, const double* gcon16, double gdet)
+{
+  Geo<double> g;
+  for (int a = 0; a < 4; a++)
+    for (int b = a; b < 4; b++) {
+      g.gcov[sym(a, b)] = gcov16[a * 4 + b];
+      g.gcon[sym(a, b)] = gcon16[a * 4 + b];
+    }
+  g.g = gdet;
+  return g;
+}
+
+double rel(double a, double b) { return fabs(a - b) / fmax(fmax(fabs(a), fabs(b)), 1e-300); }
+
+// forward functions with a scalar output <lambda, F(p)>
+double f_flux(const double* p, const Geo<double>& g, int dir, double gam, const double* lam)
+{
+  State<double> q;
+  state_of(p, g, q);
+  double F[NPR];
+  flux_of<double, false>(p, q, dir, g, gam, F);
+  double s = 0.;
+  for (int k = 0; k < NPR; k++) s += lam[k] * F[k];
+  return s;
+}
+
+double f_vchar(const double* p, const Geo<double>& g, int dir, double gam, const double* lam)
+{
+  State<double> q;
+  state_of(p, g, q);
+  double vmax, vmin;
+  vchar_of(p, q, dir, g, gam, vmax, vmin);
+  return lam[0] * vmax + lam[1] * vmin;
+}
+
+double f_limit(const double* p, const Geo<double>& g, double gmax, const double* lam)
+{
+  double pp[NPR];
+  memcpy(pp, p, sizeof(pp));
+  limit_gamma(gmax, pp, g);
+  double s = 0.;
+  for (int k = 0; k < NPR; k++) s += lam[k] * pp[k];
+  return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+// which: 0 flux (dir), 1 vchar (dir), 2 limit_gamma (gmax = aux)
+double ab_check(int which, const double* p, const double* v, const double* lam, const double* gcov16,
+                const double* gcon16, double gdet, int dir, double gam, double aux, double h)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  double pp[NPR], pm[NPR], pb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for (int k = 0; k < NPR; k++) {
+    pp[k] = p[k] + h * v[k];
+    pm[k] = p[k] - h * v[k];
+  }
+  double fd = 0.;
+  State<double> q;
+  state_of(p, g, q);
+  StateAdj qb;
+  qb.zero();
+  if (which == 0) {
+    fd = (f_flux(pp, g, dir, gam, lam) - f_flux(pm, g, dir, gam, lam)) / (2. * h);
+    adj_flux(p, q, dir, g, gam, lam, qb, pb);
+    adj_state(p, g, q, qb, pb);
+  } else if (which == 1) {
+    fd = (f_vchar(pp, g, dir, gam, lam) - f_vchar(pm, g, dir, gam, lam)) / (2. * h);
+    if (adj_vchar(p, q, dir, g, gam, lam[0], lam[1], qb, pb)) return -1.;
+    adj_state(p, g, q, qb, pb);
+  } else {
+    fd = (f_limit(pp, g, aux, lam) - f_limit(pm, g, aux, lam)) / (2. * h);
+    adj_limit_gamma(aux, p, g, lam, pb);
+  }
+  double an = 0.;
+  for (int k = 0; k < NPR; k++) an += pb[k] * v[k];
+  return rel(fd, an);
+}
+
+// one face: forward through face_flux's arithmetic (in adj_face_flux's own
+// forward part) by finite differences of <lambda, F(pl, pr)>
+static double face_value(const double* pl, const double* pr, const Geo<double>& g, int dir, double gam,
+                         double gmax, int fluxmethod, const double* lam)
+{
+  double a[NPR], b[NPR];
+  memcpy(a, pl, sizeof(a));
+  memcpy(b, pr, sizeof(b));
+  const int bd = B1 + dir - 1;
+  a[bd] = b[bd] = 0.5 * (a[bd] + b[bd]);
+  limit_gamma(gmax, a, g);
+  limit_gamma(gmax, b, g);
+  State<double> ql, qr;
+  state_of(a, g, ql);
+  state_of(b, g, qr);
+  double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+  flux_of<double, false>(a, ql, dir, g, gam, Fl);
+  flux_of<double, false>(b, qr, dir, g, gam, Fr);
+  flux_of<double, false>(a, ql, 0, g, gam, Ul);
+  flux_of<double, false>(b, qr, 0, g, gam, Ur);
+  double cxl, cnl, cxr, cnr;
+  vchar_of(a, ql, dir, g, gam, cxl, cnl);
+  vchar_of(b, qr, dir, g, gam, cxr, cnr);
+  double lmin = rmin(cnl, cnr), lmax = rmax(cxl, cxr);
+  lmin = fabs(rmax(0., -lmin));
+  lmax = fabs(rmax(0., lmax));
+  const double cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
+  const double hf = (fluxmethod == 1) ? 1.0 : 0.0, lf = (fluxmethod == 1) ? 0.0 : 1.0;
+  double s = 0.;
+  for (int k = 0; k < NPR; k++) {
+    double Fo;
+    if (cmax + cmin != 0.0)
+      Fo = hf * ((cmax * Fl[k] + cmin * Fr[k] - cmax * cmin * (Ur[k] - Ul[k])) / (cmax + cmin)) +
+           lf * (0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k])));
+    else
+      Fo = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+    s += lam[k] * Fo;
+  }
+  return s;
+}
+
+double ab_check_face(const double* pl, const double* pr, const double* vl, const double* vr, const double* lam,
+                     const double* gcov16, const double* gcon16, double gdet, int dir, double gam, double gmax,
+                     int fluxmethod, double h)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  double a[NPR], b[NPR], c[NPR], d[NPR];
+  for (int k = 0; k < NPR; k++) {
+    a[k] = pl[k] + h * vl[k];
+    b[k] = pr[k] + h * vr[k];
+    c[k] = pl[k] - h * vl[k];
+    d[k] = pr[k] - h * vr[k];
+  }
+  const double fd = (face_value(a, b, g, dir, gam, gmax, fluxmethod, lam) -
+                     face_value(c, d, g, dir, gam, gmax, fluxmethod, lam)) / (2. * h);
+  double plb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.}, prb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  if (adj_face_flux(pl, pr, g, dir, gam, gmax, fluxmethod, lam, plb, prb)) return -1.;
+  double an = 0.;
+  for (int k = 0; k < NPR; k++) an += plb[k] * vl[k] + prb[k] * vr[k];
+  return rel(fd, an);
+}
+
+// reconstruction rows against finite differences of the forward limiter
+double ab_check_recon(int para, const double* y, const double* v, double lam_l, double lam_r, double h)
+{
+  double cl[5], cr[5];
+  recon_rows(para, y, cl, cr);
+  double yp[5], ym[5];
+  for (int m = 0; m < 5; m++) {
+    yp[m] = y[m] + h * v[m];
+    ym[m] = y[m] - h * v[m];
+  }
+  double lp, rp, lm, rm;
+  if (para) {
+    para4(yp[0], yp[1], yp[2], yp[3], yp[4], lp, rp);
+    para4(ym[0], ym[1], ym[2], ym[3], ym[4], lm, rm);
+  } else {
+    double dq = mc_slope(yp[1], yp[2], yp[3]);
+    lp = yp[2] - 0.5 * dq;
+    rp = yp[2] + 0.5 * dq;
+    dq = mc_slope(ym[1], ym[2], ym[3]);
+    lm = ym[2] - 0.5 * dq;
+    rm = ym[2] + 0.5 * dq;
+  }
+  const double fd = (lam_l * (lp - lm) + lam_r * (rp - rm)) / (2. * h);
+  double an = 0.;
+  for (int m = 0; m < 5; m++) an += (lam_l * cl[m] + lam_r * cr[m]) * v[m];
+  return rel(fd, an);
+}
+
+// J_U^T x = b through primtoU_jacobian/solve_transpose8, checked as
+// <x, dU/dp v> = <b, v> with dU/dp v from finite differences of primtoU
+double ab_check_ift(const double* p, const double* v, const double* b, const double* gcov16, const double* gcon16,
+                    double gdet, double gam, double h)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  double J[NPR][NPR], x[NPR];
+  primtoU_jacobian(p, g, gam, J);
+  if (solve_transpose8(J, b, x)) return -1.;
+  double pp[NPR], pm[NPR], Up[NPR], Um[NPR];
+  for (int k = 0; k < NPR; k++) {
+    pp[k] = p[k] + h * v[k];
+    pm[k] = p[k] - h * v[k];
+  }
+  State<double> q;
+  state_of(pp, g, q);
+  flux_of<double, false>(pp, q, 0, g, gam, Up);
+  state_of(pm, g, q);
+  flux_of<double, false>(pm, q, 0, g, gam, Um);
+  double lhs = 0., rhs = 0.;
+  for (int k = 0; k < NPR; k++) {
+    lhs += x[k] * (Up[k] - Um[k]) / (2. * h);
+    rhs += b[k] * v[k];
+  }
+  return rel(lhs, rhs);
+}
+
+}  // extern "C"
