@@ -93,7 +93,7 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
            "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
            "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
-           "harm_ensemble_sync", "harm_ensemble_destroy"]
+           "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt"]
 
 
 def load_library(path=None):
@@ -136,6 +136,9 @@ def load_library(path=None):
     lib.harm_get_currents.argtypes = [vp, dp, dp, dp]
     lib.harm_write_dump.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(_DumpHeader), dp]
     lib.harm_set_tiles.argtypes = [vp, ctypes.POINTER(_Tiles)]
+    lib.harm_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp,
+                                     dp]
+    lib.harm_run_fixed_dt.argtypes = [vp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
     lib.harm_get_tiles.argtypes = [vp, ctypes.POINTER(_Tiles)]
     lib.harm_ensemble_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, vp, ctypes.POINTER(vp)]
     lib.harm_ensemble_step.argtypes = [vp, ctypes.c_int]
@@ -347,6 +350,31 @@ class HarmGPU:
         t = _Tiles()
         _check(self.lib.harm_get_tiles(self._h, ctypes.byref(t)), "harm_get_tiles")
         return (t.update_x, t.update_y), (t.small_x, t.small_y)
+
+    def adjoint(self, nsteps, checkpoint_every=16, w_mass=1.0, w_em=0.0, lam_final=None):
+        """Forward nsteps from the current state (its ghost zones first
+        refilled by the boundary conditions), then the adjoint back: returns
+        (J, dJ/dp_0 [n1m, n2m, 8] on the active zones (ghost entries 0), dt
+        sequence, (forward ms, backward ms)).  The context ends at the
+        forward run's final state."""
+        J = ctypes.c_double()
+        grad = np.zeros((self.n1m, self.n2m, NPR))
+        dts = np.zeros(int(nsteps))
+        ms = np.zeros(2)
+        lam = None if lam_final is None else np.ascontiguousarray(lam_final, dtype=np.float64)
+        _check(self.lib.harm_adjoint_run(self._h, int(nsteps), int(checkpoint_every), float(w_mass), float(w_em),
+                                         None if lam is None else _dp(lam), ctypes.byref(J), _dp(grad), _dp(dts),
+                                         _dp(ms)), "harm_adjoint_run")
+        return J.value, grad, dts, (ms[0], ms[1])
+
+    def run_fixed_dt(self, dts, w_mass=1.0, w_em=0.0, lam_final=None):
+        """The adjoint's objective for len(dts) steps with the given dt."""
+        J = ctypes.c_double()
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        lam = None if lam_final is None else np.ascontiguousarray(lam_final, dtype=np.float64)
+        _check(self.lib.harm_run_fixed_dt(self._h, _dp(d), len(d), float(w_mass), float(w_em),
+                                          None if lam is None else _dp(lam), ctypes.byref(J)), "harm_run_fixed_dt")
+        return J.value
 
     def get_fluxes(self):
         f1 = np.zeros((self.n1m, self.n2m, NPR))

@@ -71,9 +71,20 @@ template <int N>
 HD_INLINE bool operator>(const Tan<N>& a, const Tan<N>& b) { return a.v > b.v; }
 template <int N>
 HD_INLINE bool operator<=(const Tan<N>& a, const Tan<N>& b) { return a.v <= b.v; }
-using ::fabs;  // keeps fabs(double) visible next to the overload below
+using ::fabs;  // keep fabs(double), sqrt(double) visible next to the overloads below
+using ::sqrt;
 template <int N>
 HD_INLINE Tan<N> fabs(const Tan<N>& a) { return (a.v < 0.) ? -a : a; }
+template <int N>
+HD_INLINE Tan<N> sqrt(const Tan<N>& a)
+{
+  Tan<N> r;
+  r.v = sqrt(a.v);
+  for (int k = 0; k < N; k++) r.d[k] = (r.v > 0.) ? a.d[k] / (2. * r.v) : 0.;
+  return r;
+}
+template <int N>
+HD_INLINE bool operator>=(const Tan<N>& a, const Tan<N>& b) { return a.v >= b.v; }
 
 // ------------------------------------------------------------ state
 struct StateAdj {
@@ -430,6 +441,48 @@ HD_INLINE int adj_face_flux(const double* pl_in, const double* pr_in, const Geo<
   return 0;
 }
 
+// The face flux itself (the forward part of adj_face_flux), for the faces
+// where fix_flux clamps a component on its sign.  Returns the fail code.
+HD_INLINE int face_flux_primal(const double* pl_in, const double* pr_in, const Geo<double>& g, int dir, double gam,
+                               double gammamax, int fluxmethod, double* Fo)
+{
+  double la[NPR], lb[NPR];
+  const int bd = B1 + dir - 1;
+  for (int k = 0; k < NPR; k++) {
+    la[k] = pl_in[k];
+    lb[k] = pr_in[k];
+  }
+  la[bd] = lb[bd] = 0.5 * (pl_in[bd] + pr_in[bd]);
+  int rc = limit_gamma(gammamax, la, g);
+  if (!rc) rc = limit_gamma(gammamax, lb, g);
+  if (rc) return rc;
+  State<double> ql, qr;
+  state_of(la, g, ql);
+  state_of(lb, g, qr);
+  double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+  flux_of<double, false>(la, ql, dir, g, gam, Fl);
+  flux_of<double, false>(lb, qr, dir, g, gam, Fr);
+  flux_of<double, false>(la, ql, 0, g, gam, Ul);
+  flux_of<double, false>(lb, qr, 0, g, gam, Ur);
+  double cxl, cnl, cxr, cnr;
+  rc = vchar_of(la, ql, dir, g, gam, cxl, cnl);
+  if (!rc) rc = vchar_of(lb, qr, dir, g, gam, cxr, cnr);
+  if (rc) return rc;
+  double lmin = rmin(cnl, cnr), lmax = rmax(cxl, cxr);
+  lmin = fabs(rmax(0., -lmin));
+  lmax = fabs(rmax(0., lmax));
+  const double cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
+  const double hf = (fluxmethod == 1) ? 1.0 : 0.0, lf = (fluxmethod == 1) ? 0.0 : 1.0;
+  for (int k = 0; k < NPR; k++) {
+    if (cmax + cmin != 0.0)
+      Fo[k] = hf * ((cmax * Fl[k] + cmin * Fr[k] - cmax * cmin * (Ur[k] - Ul[k])) / (cmax + cmin)) +
+              lf * (0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k])));
+    else
+      Fo[k] = 0.5 * (Fl[k] + Fr[k] - ctop * (Ur[k] - Ul[k]));
+  }
+  return 0;
+}
+
 // Jacobian rows of a zone's two interface states along a direction with
 // respect to its stencil (one primitive): PARA4 uses y[-2..2], MC y[-1..1].
 // cl[m], cr[m] = d(left state)/d y[m-2], d(right state)/d y[m-2].
@@ -461,6 +514,73 @@ HD_INLINE void recon_rows(int para, const double* y, double* cl, double* cr)
       cr[m + 1] = r.d[m];
     }
   }
+}
+
+// ------------------------------------------------------------ ghost zones
+// The velocity part of an x1 ghost zone's boundary fill (bounds.fishmon.c:
+// inflow_check_rel4vel's fix, fixup.c:1784-1829, then limit_gamma) on u~
+// alone, templated for tangents; dofix is decided by the caller on the
+// values.  Returns nonzero where the forward map fails.
+template <typename T>
+HD_INLINE T gamma_T(const T* u, const double* c)
+{
+  const T q = T(c[4]) * u[0] * u[0] + T(c[7]) * u[1] * u[1] + T(c[9]) * u[2] * u[2] +
+              T(2.) * (T(c[5]) * u[0] * u[1] + T(c[6]) * u[0] * u[2] + T(c[8]) * u[1] * u[2]);
+  return sqrt(T(1.) + q);
+}
+template <typename T>
+HD_INLINE int x1_velocity_map(T* u, const Geo<double>& g, double gammamax, bool dofix)
+{
+  if (dofix) {
+    T gamma = gamma_T(u, g.gcov);
+    for (int k = 0; k < 3; k++) u[k] = u[k] / gamma;
+    const double alpha = 1. / sqrt(-g.gcon[0]);
+    const double betacon = g.gcon[1] * alpha * alpha;
+    u[0] = T(betacon / alpha);
+    T vsq = T(0.);
+    for (int jj = 1; jj < 4; jj++)
+      for (int kk = 1; kk < 4; kk++) vsq = vsq + T(g.gcov[sym(jj, kk)]) * u[jj - 1] * u[kk - 1];
+    if (vsq < T(0.0)) {
+      if (vsq > T(-DBL_EPS_REF * 100.0)) vsq = T(0.0);
+      else return FAIL_VSQ_NEG;
+    }
+    if (vsq >= T(1.0)) vsq = T(1.0 - 1.0 / (gammamax * gammamax));
+    gamma = T(1.) / sqrt(T(1.) - vsq);
+    for (int k = 0; k < 3; k++) u[k] = u[k] * gamma;
+  }
+  if (gammamax > 1.0) {
+    const T gamma = gamma_T(u, g.gcov);
+    if (gamma > T(gammamax) && gamma.v != 1.0) {
+      const T pref = (T(gammamax) * T(gammamax) - T(1.)) / (gamma * gamma - T(1.));
+      if (pref < T(0.0)) return FAIL_UTCALC_DISCR;
+      const T f = sqrt(pref);
+      for (int k = 0; k < 3; k++) u[k] = u[k] * f;
+    }
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------ source
+// The geometric source dUg[UU+l] = g sum_j sum_k T^j_k Gamma^k_{l j} of state
+// p (conn[conn_index(k, l, j)] = Gamma^k_{l j}, symmetric pair (l, j)
+// packed): dUgb (the adjoints of dUg[UU..U3]) -> pb.
+HD_INLINE void adj_source(const double* p, const Geo<double>& g, double gam, const double* conn40,
+                          const double* dUgb, double* pb)
+{
+  State<double> q;
+  state_of(p, g, q);
+  StateAdj qb;
+  qb.zero();
+  for (int jj = 0; jj < 4; jj++) {
+    double rowb[4];
+    for (int k = 0; k < 4; k++) {
+      double s = 0.;
+      for (int l = 0; l < 4; l++) s += dUgb[l] * g.g * conn40[k * 10 + sym(l, jj)];
+      rowb[k] = s;
+    }
+    adj_mhd_row(p, jj, q, gam, rowb, qb, pb);
+  }
+  adj_state(p, g, q, qb, pb);
 }
 
 // ------------------------------------------------------------ con-to-prim

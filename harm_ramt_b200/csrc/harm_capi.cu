@@ -34,6 +34,22 @@ __global__ void k_faraday(StepArgs a, const double* pv);
 __global__ void k_current(StepArgs a);
 __global__ void k_currents_commit(StepArgs a);
 __global__ void k_dump_columns(StepArgs a, const double* pv, double* out, int* nfail);
+__global__ void k_adj_seed_edot(StepArgs a, const double* pv, double* lam, double w);
+__global__ void k_adj_poledeath(StepArgs a, double* lam);
+__global__ void k_adj_ghosts(StepArgs a, double* lam, const double* src);
+__global__ void k_adj_fixup(StepArgs a, const double* lam_in, double* lam_snap, const double* snap, const int* flag,
+                            const unsigned char* fixset);
+__global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, const int* flaginv, const double* pi,
+                             double cdt, double* lam_pi, double* lam_dU);
+__global__ void k_adj_source(StepArgs a, const double* pb, const double* lam_dU, double* lam_b);
+__global__ void k_adj_corner(StepArgs a, const double* lam_dU, double* lam_e);
+__global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* lam_b,
+                            int dir, double seed_mdot);
+__global__ void k_set_dt(StepArgs a, const double* dts, int k);
+__global__ void k_get_dt(StepArgs a, double* dts, int k);
+__global__ void k_axpy(double* y, const double* x, long long n);
+__global__ void k_mask_ghosts(StepArgs a, double* lam);
+__global__ void k_dot_active(StepArgs a, const double* lam, const double* pv, double* out);
 constexpr int DUMP_DYNCOLS = 50;
 __global__ void k_ref_to_planes(StepArgs a, const double* ref, const int* refflag, double* pv);
 __global__ void k_planes_to_ref(StepArgs a, const double* pv, double* ref, int* refflag);
@@ -65,7 +81,7 @@ struct harm_ctx {
   dim3 tile_small;   // block of the stencil/fixup/boundary kernels
   StepArgs args() const
   {
-    StepArgs a;
+    StepArgs a{};
     a.gr = gr;
     a.pp.lim = cfg.lim;
     a.pp.fluxmethod = cfg.fluxmethod;
@@ -99,6 +115,8 @@ struct harm_ctx {
     a.pstep = d_p;
     a.cur = d_cur;
     a.pp.currents = cfg.currents;
+    a.rec_pinv = nullptr;
+    a.rec_fixset = nullptr;
     a.nblocks_flux = nblocks_flux;
     a.sc = d_sc;
     return a;
@@ -139,19 +157,41 @@ struct Timer {
   }
 };
 
-static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
+// What the adjoint's forward recomputation of a step keeps (per substep):
+// the inverted primitives before floors, the update's output and pflag, the
+// state after the first bound (what the repairs read), the state after the
+// repairs and the final pflag, and the neighbour set of each repair.
+struct Rec {
+  double* pn;  // the step's p
+  double* pinv[2];
+  double* upd[2];
+  double* snap[2];
+  double* pre2[2];
+  int* flaginv[2];
+  int* flag[2];
+  unsigned char* fixset[2];
+};
+
+static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullptr)
 {
   Timer dummy;
   Timer& T = tm ? *tm : dummy;
-  const StepArgs a = c->args();
+  const StepArgs a0 = c->args();
+  StepArgs a = a0;
   const int n1 = c->cfg.n1, n2 = c->cfg.n2;
   const dim3 fb(32, FLUX_BY);     // k_flux's shape is fixed by its warp/shared-memory state sharing
   const dim3 b = c->tile_small;   // the other stencil kernels
   const dim3 ub = c->tile_update;
   cudaStream_t s = c->stream;
+  const size_t pbytes = (size_t)NPR * c->gr.plane * sizeof(double), fbytes = (size_t)c->gr.plane * sizeof(int);
+  if (rec) cudaMemcpyAsync(rec->pn, c->d_p, pbytes, cudaMemcpyDeviceToDevice, s);
   k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
   T.mark(s, KC_BSQ);
   for (int sub = 0; sub < 2; sub++) {
+    if (rec) {
+      a.rec_pinv = rec->pinv[sub];
+      a.rec_fixset = rec->fixset[sub];
+    }
     const double* pi = c->d_p;
     const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
@@ -165,12 +205,17 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     T.mark(s, KC_EMF);
     launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE);
+    if (rec) {
+      cudaMemcpyAsync(rec->upd[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(rec->flaginv[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
+    }
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
     if (poledeath) {
       k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
       T.mark(s, KC_POLE);
     }
+    if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
     // force-free: no b^2 flags (so no check-solution votes) and no
     // fixup_utoprim (fixup.c:542); the second bound would repeat the first
     if (ffde) continue;
@@ -186,6 +231,10 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
     T.mark(s, KC_FIXC);
     k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_FIXA);
+    if (rec) {
+      cudaMemcpyAsync(rec->pre2[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(rec->flag[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
+    }
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 0);
     T.mark(s, KC_BOUND);
     if (poledeath) {
@@ -193,6 +242,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr)
       T.mark(s, KC_POLE);
     }
   }
+  a = a0;
   if (c->cfg.currents) {
     // step_ch.c:143-156: Faraday slots and J^mu at the new time
     k_faraday<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, c->d_p);
@@ -749,6 +799,308 @@ int harm_ensemble_sync(harm_ensemble* e, harm_status* st)
     else if (rc != HARM_OK) return rc;
   }
   return worst;
+}
+
+// ---------------------------------------------------------------- adjoint
+namespace {
+
+struct AdjWork {
+  std::vector<void*> mem;
+  Rec rec;
+  double *La, *Lc, *Lb, *Lsnap, *LdU, *Le, *dts, *dot;
+  bool ok = true;
+  void* get(size_t bytes)
+  {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      ok = false;
+      return nullptr;
+    }
+    mem.push_back(p);
+    return p;
+  }
+  ~AdjWork()
+  {
+    for (void* p : mem) cudaFree(p);
+  }
+};
+
+// the step's state the adjoint restores: p and the check-solution gamma table
+struct Saved {
+  double* p;
+  double* gc;
+};
+
+// blocks of k_dot_active (one partial sum each)
+size_t dot_blocks(const harm_ctx* c)
+{
+  const dim3 g = grid2(c->cfg.n1, c->cfg.n2, dim3(32, 4));
+  return (size_t)g.x * g.y;
+}
+
+int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps)
+{
+  const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
+  w.rec.pn = (double*)w.get(P);
+  for (int s = 0; s < 2; s++) {
+    w.rec.pinv[s] = (double*)w.get(P);
+    w.rec.upd[s] = (double*)w.get(P);
+    w.rec.snap[s] = (double*)w.get(P);
+    w.rec.pre2[s] = (double*)w.get(P);
+    w.rec.flaginv[s] = (int*)w.get(pl * sizeof(int));
+    w.rec.flag[s] = (int*)w.get(pl * sizeof(int));
+    w.rec.fixset[s] = (unsigned char*)w.get(pl);
+  }
+  w.La = (double*)w.get(P);
+  w.Lc = (double*)w.get(P);
+  w.Lb = (double*)w.get(P);
+  w.Lsnap = (double*)w.get(P);
+  w.LdU = (double*)w.get(P);
+  w.Le = (double*)w.get(pl * sizeof(double));
+  w.dts = (double*)w.get((size_t)nsteps * sizeof(double));
+  w.dot = (double*)w.get(dot_blocks(c) * sizeof(double));
+  return w.ok ? HARM_OK : HARM_ENOMEM;
+}
+
+void save_state(harm_ctx* c, const Saved& s)
+{
+  const size_t pl = (size_t)c->gr.plane;
+  cudaMemcpyAsync(s.p, c->d_p, NPR * pl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(s.gc, c->d_gammacheck, pl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+}
+
+void load_state(harm_ctx* c, const Saved& s)
+{
+  const size_t pl = (size_t)c->gr.plane;
+  cudaMemcpyAsync(c->d_p, s.p, NPR * pl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_gammacheck, s.gc, pl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+}
+
+// one substep's adjoint: lam_in (the substep output's adjoint, ghosts
+// included; consumed) -> lam_pi_acc (+=, pi), Lb (the pb adjoint, set)
+void adjoint_substep(harm_ctx* c, AdjWork& w, int sub, double* lam_in, const double* pi, const double* pb,
+                     double cdt, double seed_mdot, double* lam_pi_acc)
+{
+  const StepArgs a = c->args();
+  const int n1 = c->cfg.n1, n2 = c->cfg.n2;
+  const dim3 b(32, 4);
+  cudaStream_t s = c->stream;
+  const size_t P = (size_t)NPR * c->gr.plane * sizeof(double);
+  const Rec& r = w.rec;
+  k_adj_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, lam_in);
+  k_adj_ghosts<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, lam_in, r.pre2[sub]);
+  cudaMemsetAsync(w.Lsnap, 0, P, s);
+  k_adj_fixup<<<grid2(n1, n2, b), b, 0, s>>>(a, lam_in, w.Lsnap, r.snap[sub], r.flag[sub], r.fixset[sub]);
+  k_adj_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, w.Lsnap);
+  k_adj_ghosts<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, w.Lsnap, r.upd[sub]);
+  cudaMemsetAsync(w.Lb, 0, P, s);
+  k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], pi, cdt, lam_pi_acc, w.LdU);
+  k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, w.Lb);
+  k_adj_corner<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a, w.LdU, w.Le);
+  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lb, 1, seed_mdot);
+  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lb, 2, 0.);
+}
+
+// step n's adjoint after its recording recomputation (d_p = p^{n+1},
+// d_pk0 = the midpoint state): w.La = lambda_{n+1} -> lambda_n
+void adjoint_step(harm_ctx* c, AdjWork& w, double dtn, double wm, double we)
+{
+  const StepArgs a = c->args();
+  cudaStream_t s = c->stream;
+  const long long nval = (long long)NPR * c->gr.plane;
+  const size_t P = (size_t)nval * sizeof(double);
+  const double surface = c->cfg.dx2 * (2.0 * 3.14159265358979323846);
+  k_adj_seed_edot<<<(c->cfg.n2 + 127) / 128, 128, 0, s>>>(a, c->d_p, w.La, we * dtn);
+  cudaMemsetAsync(w.Lc, 0, P, s);
+  adjoint_substep(c, w, 1, w.La, w.rec.pn, c->d_pk0, 1.0 * dtn, wm * dtn * surface, w.Lc);
+  cudaMemcpyAsync(w.La, w.Lb, P, cudaMemcpyDeviceToDevice, s);
+  adjoint_substep(c, w, 0, w.La, w.rec.pn, w.rec.pn, 0.5 * dtn, 0., w.Lc);
+  k_axpy<<<(unsigned)((nval + 255) / 256), 256, 0, s>>>(w.Lc, w.Lb, nval);
+  cudaMemcpyAsync(w.La, w.Lc, P, cudaMemcpyDeviceToDevice, s);
+}
+
+// <lam, p> over the active zones, lam given in the reference layout (host)
+int host_lambda_to_planes(harm_ctx* c, const double* lam_host, double* planes)
+{
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  CK(cudaMemcpyAsync(c->d_stage, lam_host, (size_t)c->n1m * c->n2m * NPR * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  k_ref_to_planes<<<grid2(c->n1m, c->n2m, b), b, 0, c->stream>>>(a, c->d_stage, nullptr, planes);
+  CK(cudaGetLastError());
+  return HARM_OK;
+}
+
+int objective(harm_ctx* c, AdjWork& w, double wm, double we, bool with_lam, double* J)
+{
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  double dot = 0.;
+  std::vector<double> part(dot_blocks(c));
+  if (with_lam) {
+    k_dot_active<<<grid2(c->cfg.n1, c->cfg.n2, b), b, 0, c->stream>>>(a, w.La, c->d_p, w.dot);
+    CK(cudaMemcpyAsync(part.data(), w.dot, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (with_lam)
+    for (double x : part) dot += x;  // block partials in a fixed order: the same J on every run
+  *J = wm * h.hz[4] + we * h.hz[6] + dot;
+  return HARM_OK;
+}
+
+int zero_accumulators(harm_ctx* c)
+{
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  h.hz[4] = h.hz[5] = h.hz[6] = 0.;
+  CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  return HARM_OK;
+}
+
+// the boundary conditions applied to the input state before the first step
+// (init.fishmon.c's bound_prim after init): the adjoint's independent
+// variables are the active zones, the ghosts being theirs through this bound
+void bound_input(harm_ctx* c)
+{
+  const StepArgs a = c->args();
+  const dim3 b(32, 4);
+  k_bound<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, c->stream>>>(a, c->d_p, 1);
+  k_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, c->stream>>>(a, c->d_p);
+}
+
+bool adjoint_supported(const harm_ctx* c)
+{
+  return c->cfg.precision == HARM_PREC_FP64 && c->cfg.eom == HARM_EOM_GRMHD && c->cfg.bc == HARM_BC_TORUS;
+}
+
+}  // namespace
+
+int harm_run_fixed_dt(harm_ctx* c, const double* dts, int nsteps, double w_mass, double w_em, const double* lam_final,
+                      double* J)
+{
+  if (!c || !dts || nsteps < 1 || !J) return HARM_EINVAL;
+  if (!c->geo_ok) return HARM_EGEOMETRY;
+  if (!adjoint_supported(c)) return HARM_EINVAL;
+  AdjWork w;
+  const StepArgs a = c->args();
+  w.dts = (double*)w.get((size_t)nsteps * sizeof(double));
+  w.La = (double*)w.get((size_t)NPR * c->gr.plane * sizeof(double));
+  w.dot = (double*)w.get(dot_blocks(c) * sizeof(double));
+  if (!w.ok) return HARM_ENOMEM;
+  CK(cudaMemcpyAsync(w.dts, dts, (size_t)nsteps * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  bound_input(c);
+  int rc = zero_accumulators(c);
+  if (rc) return rc;
+  if ((rc = harm_step(c, 0)) != HARM_OK) return rc;  // capture the step graph
+  for (int n = 0; n < nsteps; n++) {
+    k_set_dt<<<1, 1, 0, c->stream>>>(a, w.dts, n);
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+  }
+  if (lam_final && (rc = host_lambda_to_planes(c, lam_final, w.La)) != HARM_OK) return rc;
+  return objective(c, w, w_mass, w_em, lam_final != nullptr, J);
+}
+
+int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mass, double w_em,
+                     const double* lam_final, double* J, double* grad, double* dts_out, double* ms_out)
+{
+  if (!c || nsteps < 1 || checkpoint_every < 1 || !J || !grad) return HARM_EINVAL;
+  if (!c->geo_ok) return HARM_EGEOMETRY;
+  if (!adjoint_supported(c)) return HARM_EINVAL;
+  AdjWork w;
+  int rc = adj_alloc(c, w, nsteps);
+  if (rc) return rc;
+  const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
+  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  std::vector<Saved> ck(nck), seg(checkpoint_every);
+  for (auto& x : ck) x = Saved{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
+  for (auto& x : seg) x = Saved{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
+  Saved fin{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
+  Saved in0{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
+  if (!w.ok) return HARM_ENOMEM;
+  const StepArgs a = c->args();
+  cudaStream_t s = c->stream;
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  save_state(c, in0);
+  bound_input(c);
+  if ((rc = zero_accumulators(c)) != HARM_OK) return rc;
+  if ((rc = harm_step(c, 0)) != HARM_OK) return rc;
+  // forward: free dt, recorded; checkpoints every checkpoint_every steps
+  CK(cudaEventRecord(e0, s));
+  for (int n = 0; n < nsteps; n++) {
+    if (n % checkpoint_every == 0) save_state(c, ck[n / checkpoint_every]);
+    k_get_dt<<<1, 1, 0, s>>>(a, w.dts, n);
+    CK(cudaGraphLaunch(c->gexec, s));
+  }
+  CK(cudaEventRecord(e1, s));
+  if (lam_final) {
+    if ((rc = host_lambda_to_planes(c, lam_final, w.La)) != HARM_OK) return rc;
+    const dim3 b(32, 4);
+    k_mask_ghosts<<<grid2(c->n1m, c->n2m, b), b, 0, s>>>(a, w.La);
+  } else {
+    CK(cudaMemsetAsync(w.La, 0, P, s));
+  }
+  if ((rc = objective(c, w, w_mass, w_em, lam_final != nullptr, J)) != HARM_OK) return rc;
+  DevScalars hfin;
+  CK(cudaMemcpyAsync(&hfin, c->d_sc, sizeof(hfin), cudaMemcpyDeviceToHost, s));
+  save_state(c, fin);
+  // reverse, segment by segment: recompute the segment's states, then each
+  // step again with recording, then its adjoint
+  for (int sg = nck - 1; sg >= 0; sg--) {
+    const int n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
+    load_state(c, ck[sg]);
+    for (int m = 0; m < len; m++) {
+      save_state(c, seg[m]);
+      if (m < len - 1) {
+        k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
+        CK(cudaGraphLaunch(c->gexec, s));
+      }
+    }
+    for (int m = len - 1; m >= 0; m--) {
+      double dtn;
+      CK(cudaMemcpyAsync(&dtn, w.dts + n0 + m, sizeof(double), cudaMemcpyDeviceToHost, s));
+      load_state(c, seg[m]);
+      k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
+      if ((rc = enqueue_step(c, nullptr, &w.rec)) != HARM_OK) return rc;
+      CK(cudaStreamSynchronize(s));
+      adjoint_step(c, w, dtn, w_mass, w_em);
+    }
+  }
+  // through the input's bound: ghost adjoints onto the active zones
+  {
+    const dim3 b(32, 4);
+    k_adj_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, s>>>(a, w.La);
+    k_adj_ghosts<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, s>>>(a, w.La, in0.p);
+  }
+  CK(cudaEventRecord(e2, s));
+  // the gradient in the reference layout
+  {
+    const dim3 b(32, 4);
+    k_planes_to_ref<<<grid2(c->n1m, c->n2m, b), b, 0, s>>>(a, w.La, c->d_stage, nullptr);
+    CK(cudaMemcpyAsync(grad, c->d_stage, (size_t)c->n1m * c->n2m * NPR * sizeof(double), cudaMemcpyDeviceToHost,
+                       s));
+  }
+  if (dts_out) CK(cudaMemcpyAsync(dts_out, w.dts, (size_t)nsteps * sizeof(double), cudaMemcpyDeviceToHost, s));
+  // leave the context at the forward run's end
+  load_state(c, fin);
+  CK(cudaMemcpyAsync(c->d_sc, &hfin, sizeof(hfin), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  if (ms_out) {
+    float f = 0.f, r = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventElapsedTime(&r, e1, e2);
+    ms_out[0] = f;
+    ms_out[1] = r;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  return HARM_OK;
 }
 
 int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)

@@ -52,7 +52,8 @@ struct DevScalars {
   int chk_changed[8];    // per-round change flags of the check-solution sweep
   int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
   int fixups;            // zones repaired by fixup_utoprim since the last harm_set_time
-  double hz[6];          // horizon accounting of the last step (see k_horizon)
+  double hz[7];          // horizon accounting of the last step (see k_horizon); hz[6]:
+                         // sum of dt (b^2 u^r u_t - b^r b_t) terms since the last harm_set_time
   int ndeferred;         // zones whose inversion went to the tail kernel (this substep)
   int ndeferred_total;   // same, summed since the last harm_set_time
   int cur_ring;          // currents: ring level holding the newest F^{i t}
@@ -78,6 +79,8 @@ struct StepArgs {
   int* worklist;         // deferred zone indices (capacity: one plane)
   const double* pstep;   // the step's p (the star's inner ghost field is held at it)
   double* cur;           // currents (25 planes): F^{i t} ring 3x3, F^{i r} 3, F^{i h} 3, fcon 6, jcon 4
+  double* rec_pinv;      // adjoint recording (or null): inverted prims before the floors, 8 planes
+  unsigned char* rec_fixset;  // adjoint recording (or null): neighbour set of each repaired zone
   int nblocks_flux;
   DevScalars* sc;
 };

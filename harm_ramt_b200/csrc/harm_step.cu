@@ -372,17 +372,27 @@ __global__ void k_fixup_compute(StepArgs a, const double* __restrict__ pv)
   load_geo(a, CENT, z, g);
   double gamma = gamma_of(pr, g);
   if (gamma > a.pp.gammamax) gamma = a.pp.gammamax;
+  // neighbour set (recorded for the adjoint): 0 the four faces, 1 the four
+  // corners, 2 x2 pair, 3 x1 pair, 4 and 5 the diagonal pairs, 6 + m the
+  // first good single neighbour m, 14 the all-neighbour fallback
+  int set;
   if (good(i, j + 1) && good(i, j - 1) && good(i + 1, j) && good(i - 1, j)) {
+    set = 0;
     for (int k = 0; k <= U3; k++) pr[k] = 0.25 * (P(i, j + 1, k) + P(i, j - 1, k) + P(i - 1, j, k) + P(i + 1, j, k));
   } else if (good(i + 1, j + 1) && good(i + 1, j - 1) && good(i - 1, j + 1) && good(i - 1, j - 1)) {
+    set = 1;
     for (int k = 0; k <= U3; k++) pr[k] = 0.25 * (P(i + 1, j + 1, k) + P(i + 1, j - 1, k) + P(i - 1, j + 1, k) + P(i - 1, j - 1, k));
   } else if (good(i, j + 1) && good(i, j - 1)) {
+    set = 2;
     for (int k = 0; k <= U3; k++) pr[k] = 0.5 * (P(i, j + 1, k) + P(i, j - 1, k));
   } else if (good(i + 1, j) && good(i - 1, j)) {
+    set = 3;
     for (int k = 0; k <= U3; k++) pr[k] = 0.5 * (P(i + 1, j, k) + P(i - 1, j, k));
   } else if (good(i + 1, j + 1) && good(i - 1, j - 1)) {
+    set = 4;
     for (int k = 0; k <= U3; k++) pr[k] = 0.5 * (P(i + 1, j + 1, k) + P(i - 1, j - 1, k));
   } else if (good(i + 1, j - 1) && good(i - 1, j + 1)) {
+    set = 5;
     for (int k = 0; k <= U3; k++) pr[k] = 0.5 * (P(i + 1, j - 1, k) + P(i - 1, j + 1, k));
   } else {
     const int oi[8] = {1, 1, 1, 0, -1, -1, -1, 0};
@@ -391,13 +401,16 @@ __global__ void k_fixup_compute(StepArgs a, const double* __restrict__ pv)
     for (; m < 8; m++)
       if (good(i + oi[m], j + oj[m])) break;
     if (m < 8) {
+      set = 6 + m;
       for (int k = 0; k <= U3; k++) pr[k] = P(i + oi[m], j + oj[m], k);
     } else {
+      set = 14;
       for (int k = 0; k <= U3; k++)
         pr[k] = 0.5 * (0.25 * (P(i, j + 1, k) + P(i, j - 1, k) + P(i - 1, j, k) + P(i + 1, j, k)) +
                        0.25 * (P(i + 1, j + 1, k) + P(i + 1, j - 1, k) + P(i - 1, j + 1, k) + P(i - 1, j - 1, k)));
     }
   }
+  if (a.rec_fixset) a.rec_fixset[z] = (unsigned char)set;
   int rc = limit_gamma(gamma, pr, g);
   if (rc) report_fail(a.sc, rc, i, j);
 #pragma unroll

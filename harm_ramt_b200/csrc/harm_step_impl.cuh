@@ -221,6 +221,10 @@ __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>
                                             int pfl, double* pf)
 {
   const long long pl = a.gr.plane;
+  if (a.rec_pinv) {
+#pragma unroll
+    for (int k = 0; k < NPR; k++) a.rec_pinv[k * pl + z] = pfz[k];
+  }
   a.pflag[z] = pfl;
   const double frho = __ldg(a.geo + (long long)GEO_FLOOR * pl + z), fu = __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z);
   if (frho > pfz[RHO]) pfz[RHO] = frho;
@@ -400,6 +404,7 @@ __global__ void __launch_bounds__(1024) k_horizon(StepArgs a, const double* __re
     for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
     sc->hz[4] += acc[0] * sc->dt;
     sc->hz[5] += acc[1] * sc->dt;
+    sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
   }
 }
 

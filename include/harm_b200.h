@@ -216,6 +216,43 @@ int harm_ensemble_step(harm_ensemble* e, int nsteps);
 int harm_ensemble_sync(harm_ensemble* e, harm_status* st);
 void harm_ensemble_destroy(harm_ensemble* e);
 
+/* Reverse mode (FP64, GRMHD, torus boundaries).  The objective of a run of
+   nsteps steps from the context's state p_0 is
+     J = w_mass sum_n dt_n mdot_n + w_em sum_n dt_n edot_n + <lam_final, p_N>
+   with mdot_n, edot_n the horizon mass flux and EM energy flux terms of
+   diag_flux() (harm_get_horizon: pdot[X1DN][RHO] and pdotterms 3 + 6 of UU)
+   and lam_final (reference layout [n1m][n2m][8], may be NULL) weighting the
+   active zones of the final state.  dt_n is held at the run's own values
+   (the derivative does not follow the Courant minimum).
+
+   Both first fill the ghost zones of p_0 from its active zones by the
+   boundary conditions (bound_prim after init, init.fishmon.c); on a state
+   left by a step this changes nothing but the inflow-checked x1 ghosts of
+   the two POLEDEATH rows, which then see their row's zeroed u~2.  The
+   independent variables are therefore the active zones: the ghost copies
+   put the MC/PARA4 limiters at their kinks (equal neighbours), where only
+   derivatives along the bound's own dependence exist.
+
+   harm_adjoint_run: runs the nsteps forward (free dt, recorded in dts_out
+   if not NULL), keeping a checkpoint every checkpoint_every steps, then the
+   adjoint back to p_0: grad [n1m][n2m][8] = dJ/dp_0 on the active zones
+   (ghost entries 0).  Each backward step recomputes its forward
+   step from the segment's states (recording the intermediate states, the
+   inversion flags and the repair choices) and runs the adjoint kernels:
+   floors and Lorentz limits, the con-to-prim inverse through the implicit
+   function theorem on its Jacobian, the conserved update and geometric
+   source, flux-CT, the face fluxes (HLL/LAXF, wavespeeds, states) and the
+   MC/PARA4 reconstructions differentiated piecewise, the repairs and the
+   boundary fills.  The context is left at p_N.  ms_out (may be NULL): the
+   forward and the backward wall times on the device.
+
+   harm_run_fixed_dt: the same objective for nsteps steps with dt_n given
+   (e.g. for finite differences against the adjoint). */
+int harm_adjoint_run(harm_ctx* ctx, int nsteps, int checkpoint_every, double w_mass, double w_em,
+                     const double* lam_final, double* J, double* grad, double* dts_out, double* ms_out);
+int harm_run_fixed_dt(harm_ctx* ctx, const double* dts, int nsteps, double w_mass, double w_em,
+                      const double* lam_final, double* J);
+
 /* Diagnostics: runs one step outside the graph with a CUDA event after
    every kernel and returns, per kernel class (harm_kernel_name(k), k <
    HARM_NKERNELS), the summed device time in ms and the launch count. */

@@ -24,7 +24,15 @@ Geo<double> geo_of(const double* gcov16, const double* gcon16, double gdet)
   return g;
 }
 
-double rel(double a, double b) { return fabs(a - b) / fmax(fmax(fabs(a), fabs(b)), 1e-300); }
+// the last check's two directional derivatives (finite difference, adjoint)
+double last_fd = 0., last_an = 0.;
+
+double rel(double a, double b)
+{
+  last_fd = a;
+  last_an = b;
+  return fabs(a - b) / fmax(fmax(fabs(a), fabs(b)), 1e-300);
+}
 
 // forward functions with a scalar output <lambda, F(p)>
 double f_flux(const double* p, const Geo<double>& g, int dir, double gam, const double* lam)
@@ -60,6 +68,12 @@ double f_limit(const double* p, const Geo<double>& g, double gmax, const double*
 }  // namespace
 
 extern "C" {
+
+void ab_last(double* out)
+{
+  out[0] = last_fd;
+  out[1] = last_an;
+}
 
 // which: 0 flux (dir), 1 vchar (dir), 2 limit_gamma (gmax = aux)
 double ab_check(int which, const double* p, const double* v, const double* lam, const double* gcov16,
@@ -155,6 +169,43 @@ double ab_check_face(const double* pl, const double* pr, const double* vl, const
   return rel(fd, an);
 }
 
+// the geometric source block: <lam, dUg(p)> (as k_update forms dUg)
+static double source_value(const double* p, const Geo<double>& g, double gam, const double* conn40, const double* lam)
+{
+  State<double> q;
+  state_of(p, g, q);
+  double acc[4] = {0., 0., 0., 0.};
+  for (int jj = 0; jj < 4; jj++) {
+    double row[4];
+    mhd_row<double, false>(p, jj, q, gam, row);
+    for (int l = 0; l < 4; l++)
+      for (int k = 0; k < 4; k++) acc[l] += row[k] * conn40[k * 10 + sym(l, jj)];
+  }
+  double s = 0.;
+  for (int l = 0; l < 4; l++) s += lam[l] * (0. + g.g * acc[l]);
+  return s;
+}
+
+double ab_check_source(const double* p, const double* v, const double* lam, const double* gcov16, const double* gcon16,
+                       double gdet, const double* conn64, double gam, double h)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  double conn40[40];
+  for (int k = 0; k < 4; k++)
+    for (int l = 0; l < 4; l++)
+      for (int j = l; j < 4; j++) conn40[k * 10 + sym(l, j)] = conn64[(k * 4 + l) * 4 + j];
+  double pp[NPR], pm[NPR], pb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for (int k = 0; k < NPR; k++) {
+    pp[k] = p[k] + h * v[k];
+    pm[k] = p[k] - h * v[k];
+  }
+  const double fd = (source_value(pp, g, gam, conn40, lam) - source_value(pm, g, gam, conn40, lam)) / (2. * h);
+  adj_source(p, g, gam, conn40, lam, pb);
+  double an = 0.;
+  for (int k = 0; k < NPR; k++) an += pb[k] * v[k];
+  return rel(fd, an);
+}
+
 // reconstruction rows against finite differences of the forward limiter
 double ab_check_recon(int para, const double* y, const double* v, double lam_l, double lam_r, double h)
 {
@@ -208,6 +259,38 @@ double ab_check_ift(const double* p, const double* v, const double* b, const dou
     rhs += b[k] * v[k];
   }
   return rel(lhs, rhs);
+}
+
+// the evolved conserved vector of p and its Jacobian dU/dp (row-major 8x8)
+void ab_primtoU(const double* p, const double* gcov16, const double* gcon16, double gdet, double gam, double* U,
+                double* J64)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  State<double> q;
+  state_of(p, g, q);
+  flux_of<double, false>(p, q, 0, g, gam, U);
+  if (J64) {
+    double J[NPR][NPR];
+    primtoU_jacobian(p, g, gam, J);
+    for (int r = 0; r < NPR; r++)
+      for (int c = 0; c < NPR; c++) J64[r * NPR + c] = J[r][c];
+  }
+}
+
+// the geometric source dUg[UU..U3] of p as k_update forms it
+void ab_source(const double* p, const double* gcov16, const double* gcon16, double gdet, const double* conn64,
+               double gam, double* out4)
+{
+  const Geo<double> g = geo_of(gcov16, gcon16, gdet);
+  double conn40[40];
+  for (int k = 0; k < 4; k++)
+    for (int l = 0; l < 4; l++)
+      for (int j = l; j < 4; j++) conn40[k * 10 + sym(l, j)] = conn64[(k * 4 + l) * 4 + j];
+  for (int l = 0; l < 4; l++) {
+    double lam[4] = {0., 0., 0., 0.};
+    lam[l] = 1.;
+    out4[l] = source_value(p, g, gam, conn40, lam);
+  }
 }
 
 }  // extern "C"

@@ -38,6 +38,8 @@ def _lib():
     lib.ab_check_face.argtypes = [P, P, P, P, P, P, P, d, i, d, d, i, d]
     lib.ab_check_recon.restype = d
     lib.ab_check_recon.argtypes = [i, P, P, d, d, d]
+    lib.ab_check_source.restype = d
+    lib.ab_check_source.argtypes = [P, P, P, P, P, d, P, d, d]
     lib.ab_check_ift.restype = d
     lib.ab_check_ift.argtypes = [P, P, P, P, P, d, d, d]
     return lib
@@ -149,6 +151,23 @@ def test_reconstruction_rows(para):
         err = min(lib.ab_check_recon(para, a[0][1], a[1][1], ll, lr, h) for h in HS)
         worst = max(worst, err)
     assert worst < 1e-6, worst
+
+
+def test_geometric_source_adjoint(torus_zones):
+    lib = _lib()
+    p, geom, zones = torus_zones
+    rng = np.random.default_rng(19)
+    worst = 0.0
+    for (i, j) in zones + [(3, 5), (3, 30), (4, 3), (40, 3)]:
+        pz, gc, gn, gd = _zone(p, geom, i, j)
+        conn = geom["conn"][i, j].copy()
+        v = rng.standard_normal(8) * np.abs(pz)
+        lam = rng.standard_normal(4)
+        a = [_p(x) for x in (pz, v, lam, gc, gn, conn)]
+        err = min(lib.ab_check_source(a[0][1], a[1][1], a[2][1], a[3][1], a[4][1], gd, a[5][1], 4.0 / 3.0, h)
+                  for h in HS)
+        worst = max(worst, err)
+    assert worst < TOL, worst
 
 
 def test_inverse_jacobian_solve(torus_zones):
