@@ -34,11 +34,13 @@ __device__ __forceinline__ bool active(const StepArgs& a, int i, int j)
 
 }  // namespace
 
-// edot seed: d/dp of w (b^2 u^r u_t - b^r b_t) sqrt(-g) dx2 2pi at the zones
-// (0, j) of the step's final state (diag_flux's EM terms, as k_horizon forms)
-__global__ void k_adj_seed_edot(StepArgs a, const double* __restrict__ pv, double* lam, double w)
+// edot seed: d/dp of w dt (b^2 u^r u_t - b^r b_t) sqrt(-g) dx2 2pi at the
+// zones (0, j) of the step's final state (diag_flux's EM terms, as k_horizon
+// forms); dt is the step's (a.sc->dt)
+__global__ void k_adj_seed_edot(StepArgs a, const double* __restrict__ pv, double* lam, double wfac)
 {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const double w = wfac * a.sc->dt;
   if (j >= a.gr.n2 || w == 0.) return;
   const long long pl = a.gr.plane, z = a.gr.at(0, j);
   double p[NPR];
@@ -221,18 +223,20 @@ __global__ void k_adj_fixup(StepArgs a, const double* __restrict__ lam_in, doubl
 }
 
 // The zone update: lam (adjoint of the update's output) -> lam_pi (+= own
-// zone, from U(pi)), lam_dU (= c dt Ubar, for the fluxes and the source).
+// zone, from U(pi)), lam_dU (= c dt Ubar, for the fluxes and the source;
+// c = cfac, dt the step's a.sc->dt).
 // pinv: the inverted primitives before floors; flaginv: the inversion's
 // pflag.  The geometric source's adjoint is k_adj_source's: built into this
 // kernel (after the con-to-prim Jacobian), sm_100a code of nvcc 12.9 gave
 // source adjoints that differ from the same function's host build and from
 // finite differences, at any ptxas optimisation level.
 __global__ void k_adj_update(StepArgs a, const double* __restrict__ lam, const double* __restrict__ pinv,
-                             const int* __restrict__ flaginv, const double* __restrict__ pi, double cdt,
+                             const int* __restrict__ flaginv, const double* __restrict__ pi, double cfac,
                              double* lam_pi, double* lam_dU)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (!active(a, i, j)) return;
+  const double cdt = cfac * a.sc->dt;
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
   Geo<double> g;
   load_geo(a, CENT, z, g);
@@ -256,9 +260,7 @@ __global__ void k_adj_update(StepArgs a, const double* __restrict__ lam, const d
     adj_limit_gamma(a.pp.gammamax, pfl, g, lp, l1);
     if (crho) l1[RHO] = 0.;
     if (cu) l1[UU] = 0.;
-    double J[NPR][NPR];
-    primtoU_jacobian(p1, g, gam, J);
-    if (solve_transpose8(J, l1, Ub))
+    if (ift_solve(p1, g, gam, l1, Ub))
       for (int k = 0; k < NPR; k++) Ub[k] = 0.;
   }
   // Uf = U(pi) + cdt (dUr + dUg)
@@ -319,12 +321,13 @@ __global__ void k_adj_corner(StepArgs a, const double* __restrict__ lam_dU, doub
 }
 
 // One face direction: the face-flux adjoint (from lam_dU of the two zones,
-// the EMF adjoints of its corners, and a seed on the x1 mass flux at i = 0),
-// fix_flux's zeroed components, then the face and the two reconstructions,
-// scattered onto lam_b at the stencil zones.
+// the EMF adjoints of its corners, and a seed seed_fac dt on the x1 mass flux
+// at i = 0), fix_flux's zeroed components, then the face and the two
+// reconstructions, scattered onto lam_b at the stencil zones.
 __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const double* __restrict__ lam_dU,
-                            const double* __restrict__ lam_e, double* lam_b, int dir, double seed_mdot)
+                            const double* __restrict__ lam_e, double* lam_b, int dir, double seed_fac)
 {
+  const double seed_mdot = seed_fac * a.sc->dt;
   const int i = blockIdx.x * blockDim.x + threadIdx.x - (dir == 2 ? 1 : 0);
   const int j = blockIdx.y * blockDim.y + threadIdx.y - (dir == 1 ? 1 : 0);
   const int n1 = a.gr.n1, n2 = a.gr.n2;

@@ -585,12 +585,13 @@ HD_INLINE void adj_source(const double* p, const Geo<double>& g, double gam, con
 
 // ------------------------------------------------------------ con-to-prim
 // dU/dp of the evolved conserved vector (primtoU with sqrt(-g) and the rest
-// mass in UU) at p: J[r][c] = dU_r / dp_c, by one reverse sweep per row.
-HD_INLINE void primtoU_jacobian(const double* p, const Geo<double>& g, double gam, double J[NPR][NPR])
+// mass in UU) at p, rows 0..4 (rho u^t, T^t_t + rho u^t, T^t_i): J[r][c] =
+// dU_r / dp_c, by one reverse sweep per row.  Rows B1..B3 are U_B = g B.
+HD_INLINE void primtoU_jacobian5(const double* p, const Geo<double>& g, double gam, double J[5][NPR])
 {
   State<double> q;
   state_of(p, g, q);
-  for (int r = 0; r < NPR; r++) {
+  for (int r = 0; r < 5; r++) {
     double Fb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
     Fb[r] = 1.;
     StateAdj qb;
@@ -602,35 +603,46 @@ HD_INLINE void primtoU_jacobian(const double* p, const Geo<double>& g, double ga
   }
 }
 
-// Solves J^T x = b (8 x 8, Gaussian elimination with partial pivoting on the
-// transposed matrix).  Returns nonzero for a singular matrix.
-HD_INLINE int solve_transpose8(double J[NPR][NPR], const double* b, double* x)
+// Solves dU/dp^T x = b at p (the implicit-function-theorem step of the
+// con-to-prim adjoint).  dU/dp is block triangular: U_B = g B does not
+// depend on rho..u3, so the rho..u3 columns give a 5 x 5 system in x_0..4
+// (Gaussian elimination with partial pivoting) and the B columns then give
+// x_B = (b_B - sum_r J[r][B] x_r) / g.  Returns nonzero for a singular
+// matrix.
+HD_INLINE int ift_solve(const double* p, const Geo<double>& g, double gam, const double* b, double* x)
 {
-  double A[NPR][NPR + 1];
-  for (int r = 0; r < NPR; r++) {
-    for (int c = 0; c < NPR; c++) A[r][c] = J[c][r];
-    A[r][NPR] = b[r];
+  double J[5][NPR];
+  primtoU_jacobian5(p, g, gam, J);
+  double A[5][6];
+  for (int r = 0; r < 5; r++) {
+    for (int c = 0; c < 5; c++) A[r][c] = J[c][r];
+    A[r][5] = b[r];
   }
-  for (int col = 0; col < NPR; col++) {
+  for (int col = 0; col < 5; col++) {
     int piv = col;
-    for (int r = col + 1; r < NPR; r++)
+    for (int r = col + 1; r < 5; r++)
       if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
     if (A[piv][col] == 0.0) return 1;
     if (piv != col)
-      for (int c = 0; c <= NPR; c++) {
+      for (int c = 0; c < 6; c++) {
         const double t = A[col][c];
         A[col][c] = A[piv][c];
         A[piv][c] = t;
       }
-    for (int r = col + 1; r < NPR; r++) {
+    for (int r = col + 1; r < 5; r++) {
       const double f = A[r][col] / A[col][col];
-      for (int c = col; c <= NPR; c++) A[r][c] -= f * A[col][c];
+      for (int c = col; c < 6; c++) A[r][c] -= f * A[col][c];
     }
   }
-  for (int r = NPR - 1; r >= 0; r--) {
-    double s = A[r][NPR];
-    for (int c = r + 1; c < NPR; c++) s -= A[r][c] * x[c];
+  for (int r = 4; r >= 0; r--) {
+    double s = A[r][5];
+    for (int c = r + 1; c < 5; c++) s -= A[r][c] * x[c];
     x[r] = s / A[r][r];
+  }
+  for (int c = B1; c <= B3; c++) {
+    double s = b[c];
+    for (int r = 0; r < 5; r++) s -= J[r][c] * x[r];
+    x[c] = s / g.g;
   }
   return 0;
 }

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <string>
 #include <thread>
+#include <functional>
 #include <vector>
 
 #include "../../include/harm_b200.h"
@@ -34,17 +35,17 @@ __global__ void k_faraday(StepArgs a, const double* pv);
 __global__ void k_current(StepArgs a);
 __global__ void k_currents_commit(StepArgs a);
 __global__ void k_dump_columns(StepArgs a, const double* pv, double* out, int* nfail);
-__global__ void k_adj_seed_edot(StepArgs a, const double* pv, double* lam, double w);
+__global__ void k_adj_seed_edot(StepArgs a, const double* pv, double* lam, double wfac);
 __global__ void k_adj_poledeath(StepArgs a, double* lam);
 __global__ void k_adj_ghosts(StepArgs a, double* lam, const double* src);
 __global__ void k_adj_fixup(StepArgs a, const double* lam_in, double* lam_snap, const double* snap, const int* flag,
                             const unsigned char* fixset);
 __global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, const int* flaginv, const double* pi,
-                             double cdt, double* lam_pi, double* lam_dU);
+                             double cfac, double* lam_pi, double* lam_dU);
 __global__ void k_adj_source(StepArgs a, const double* pb, const double* lam_dU, double* lam_b);
 __global__ void k_adj_corner(StepArgs a, const double* lam_dU, double* lam_e);
 __global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* lam_b,
-                            int dir, double seed_mdot);
+                            int dir, double seed_fac);
 __global__ void k_set_dt(StepArgs a, const double* dts, int k);
 __global__ void k_get_dt(StepArgs a, double* dts, int k);
 __global__ void k_axpy(double* y, const double* x, long long n);
@@ -163,6 +164,7 @@ struct Timer {
 // repairs and the final pflag, and the neighbour set of each repair.
 struct Rec {
   double* pn;  // the step's p
+  double* ph;  // the midpoint state (pk[0]) the second substep reads
   double* pinv[2];
   double* upd[2];
   double* snap[2];
@@ -243,6 +245,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     }
   }
   a = a0;
+  if (rec) cudaMemcpyAsync(rec->ph, c->d_pk0, pbytes, cudaMemcpyDeviceToDevice, s);
   if (c->cfg.currents) {
     // step_ch.c:143-156: Faraday slots and J^mu at the new time
     k_faraday<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, c->d_p);
@@ -806,7 +809,10 @@ namespace {
 
 struct AdjWork {
   std::vector<void*> mem;
-  Rec rec;
+  std::vector<Rec> rec;        // one per step of a checkpoint segment
+  std::vector<double*> pnext;  // the state after each slot's step (the next slot's pn; an extra one at the end)
+  std::vector<cudaGraphExec_t> recg;  // the recording step of each slot, captured
+  std::vector<cudaGraphExec_t> adjg;  // the adjoint step of each slot, captured
   double *La, *Lc, *Lb, *Lsnap, *LdU, *Le, *dts, *dot;
   bool ok = true;
   void* get(size_t bytes)
@@ -821,6 +827,10 @@ struct AdjWork {
   }
   ~AdjWork()
   {
+    for (cudaGraphExec_t g : recg)
+      if (g) cudaGraphExecDestroy(g);
+    for (cudaGraphExec_t g : adjg)
+      if (g) cudaGraphExecDestroy(g);
     for (void* p : mem) cudaFree(p);
   }
 };
@@ -838,19 +848,27 @@ size_t dot_blocks(const harm_ctx* c)
   return (size_t)g.x * g.y;
 }
 
-int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps)
+// nslots: steps per checkpoint segment.  Each keeps its own record, about
+// 10 state-sized arrays: a 16-step segment of a 512^2 grid holds ~3 GB.
+int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps, int nslots)
 {
   const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
-  w.rec.pn = (double*)w.get(P);
-  for (int s = 0; s < 2; s++) {
-    w.rec.pinv[s] = (double*)w.get(P);
-    w.rec.upd[s] = (double*)w.get(P);
-    w.rec.snap[s] = (double*)w.get(P);
-    w.rec.pre2[s] = (double*)w.get(P);
-    w.rec.flaginv[s] = (int*)w.get(pl * sizeof(int));
-    w.rec.flag[s] = (int*)w.get(pl * sizeof(int));
-    w.rec.fixset[s] = (unsigned char*)w.get(pl);
+  w.rec.resize(nslots);
+  for (Rec& r : w.rec) {
+    r.pn = (double*)w.get(P);
+    r.ph = (double*)w.get(P);
+    for (int s = 0; s < 2; s++) {
+      r.pinv[s] = (double*)w.get(P);
+      r.upd[s] = (double*)w.get(P);
+      r.snap[s] = (double*)w.get(P);
+      r.pre2[s] = (double*)w.get(P);
+      r.flaginv[s] = (int*)w.get(pl * sizeof(int));
+      r.flag[s] = (int*)w.get(pl * sizeof(int));
+      r.fixset[s] = (unsigned char*)w.get(pl);
+    }
   }
+  double* plast = (double*)w.get(P);
+  for (int m = 0; m < nslots; m++) w.pnext.push_back(m + 1 < nslots ? w.rec[m + 1].pn : plast);
   w.La = (double*)w.get(P);
   w.Lc = (double*)w.get(P);
   w.Lb = (double*)w.get(P);
@@ -877,46 +895,67 @@ void load_state(harm_ctx* c, const Saved& s)
 }
 
 // one substep's adjoint: lam_in (the substep output's adjoint, ghosts
-// included; consumed) -> lam_pi_acc (+=, pi), Lb (the pb adjoint, set)
-void adjoint_substep(harm_ctx* c, AdjWork& w, int sub, double* lam_in, const double* pi, const double* pb,
-                     double cdt, double seed_mdot, double* lam_pi_acc)
+// included; consumed) -> lam_pi_acc (+=, pi), out (the pb adjoint, set).
+// The update's c dt is cfac times the step's dt (a.sc->dt).
+void adjoint_substep(harm_ctx* c, AdjWork& w, const Rec& r, int sub, double* lam_in, double* out, const double* pi,
+                     const double* pb, double cfac, double seed_fac, double* lam_pi_acc)
 {
   const StepArgs a = c->args();
   const int n1 = c->cfg.n1, n2 = c->cfg.n2;
   const dim3 b(32, 4);
   cudaStream_t s = c->stream;
   const size_t P = (size_t)NPR * c->gr.plane * sizeof(double);
-  const Rec& r = w.rec;
   k_adj_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, lam_in);
   k_adj_ghosts<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, lam_in, r.pre2[sub]);
   cudaMemsetAsync(w.Lsnap, 0, P, s);
   k_adj_fixup<<<grid2(n1, n2, b), b, 0, s>>>(a, lam_in, w.Lsnap, r.snap[sub], r.flag[sub], r.fixset[sub]);
   k_adj_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, w.Lsnap);
   k_adj_ghosts<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, w.Lsnap, r.upd[sub]);
-  cudaMemsetAsync(w.Lb, 0, P, s);
-  k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], pi, cdt, lam_pi_acc, w.LdU);
-  k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, w.Lb);
+  cudaMemsetAsync(out, 0, P, s);
+  k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], pi, cfac, lam_pi_acc, w.LdU);
+  k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, out);
   k_adj_corner<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a, w.LdU, w.Le);
-  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lb, 1, seed_mdot);
-  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lb, 2, 0.);
+  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, out, 1, seed_fac);
+  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, out, 2, 0.);
 }
 
-// step n's adjoint after its recording recomputation (d_p = p^{n+1},
-// d_pk0 = the midpoint state): w.La = lambda_{n+1} -> lambda_n
-void adjoint_step(harm_ctx* c, AdjWork& w, double dtn, double wm, double we)
+// step n's adjoint from its record r and its output state pout (p^{n+1}),
+// dt the step's (a.sc->dt): w.La = lambda_{n+1} -> lambda_n.  Fixed roles
+// (La in and out, Lb the midpoint state's adjoint, Lc the accumulator), so
+// that a slot's adjoint step can be captured once and replayed.
+void adjoint_step(harm_ctx* c, AdjWork& w, const Rec& r, const double* pout, double wm, double we)
 {
   const StepArgs a = c->args();
   cudaStream_t s = c->stream;
   const long long nval = (long long)NPR * c->gr.plane;
   const size_t P = (size_t)nval * sizeof(double);
   const double surface = c->cfg.dx2 * (2.0 * 3.14159265358979323846);
-  k_adj_seed_edot<<<(c->cfg.n2 + 127) / 128, 128, 0, s>>>(a, c->d_p, w.La, we * dtn);
+  k_adj_seed_edot<<<(c->cfg.n2 + 127) / 128, 128, 0, s>>>(a, pout, w.La, we);
   cudaMemsetAsync(w.Lc, 0, P, s);
-  adjoint_substep(c, w, 1, w.La, w.rec.pn, c->d_pk0, 1.0 * dtn, wm * dtn * surface, w.Lc);
-  cudaMemcpyAsync(w.La, w.Lb, P, cudaMemcpyDeviceToDevice, s);
-  adjoint_substep(c, w, 0, w.La, w.rec.pn, w.rec.pn, 0.5 * dtn, 0., w.Lc);
-  k_axpy<<<(unsigned)((nval + 255) / 256), 256, 0, s>>>(w.Lc, w.Lb, nval);
-  cudaMemcpyAsync(w.La, w.Lc, P, cudaMemcpyDeviceToDevice, s);
+  adjoint_substep(c, w, r, 1, w.La, w.Lb, r.pn, r.ph, 1.0, wm * surface, w.Lc);
+  adjoint_substep(c, w, r, 0, w.Lb, w.La, r.pn, r.pn, 0.5, 0., w.Lc);
+  k_axpy<<<(unsigned)((nval + 255) / 256), 256, 0, s>>>(w.La, w.Lc, nval);
+}
+
+// captures what `enqueue` issues on c's stream into a graph (on a private
+// stream) and instantiates it
+int capture_graph(harm_ctx* c, const std::function<int(harm_ctx*)>& enqueue, cudaGraphExec_t* out)
+{
+  cudaStream_t cap;
+  CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  harm_ctx tmp = *c;
+  tmp.stream = cap;
+  int rc = HARM_OK;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = HARM_ECUDA;
+  if (rc == HARM_OK) {
+    rc = enqueue(&tmp);
+    if (cudaStreamEndCapture(cap, &g) != cudaSuccess) rc = HARM_ECUDA;
+  }
+  cudaStreamDestroy(cap);
+  if (rc == HARM_OK && cudaGraphInstantiate(out, g, 0) != cudaSuccess) rc = HARM_ECUDA;
+  if (g) cudaGraphDestroy(g);
+  return rc;
 }
 
 // <lam, p> over the active zones, lam given in the reference layout (host)
@@ -1010,13 +1049,12 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   if (!c->geo_ok) return HARM_EGEOMETRY;
   if (!adjoint_supported(c)) return HARM_EINVAL;
   AdjWork w;
-  int rc = adj_alloc(c, w, nsteps);
+  int rc = adj_alloc(c, w, nsteps, std::min(checkpoint_every, nsteps));
   if (rc) return rc;
   const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
   const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  std::vector<Saved> ck(nck), seg(checkpoint_every);
+  std::vector<Saved> ck(nck);
   for (auto& x : ck) x = Saved{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
-  for (auto& x : seg) x = Saved{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
   Saved fin{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
   Saved in0{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
   if (!w.ok) return HARM_ENOMEM;
@@ -1049,26 +1087,38 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   DevScalars hfin;
   CK(cudaMemcpyAsync(&hfin, c->d_sc, sizeof(hfin), cudaMemcpyDeviceToHost, s));
   save_state(c, fin);
-  // reverse, segment by segment: recompute the segment's states, then each
-  // step again with recording, then its adjoint
+  // reverse, segment by segment: recompute the segment from its checkpoint,
+  // recording every step, then the steps' adjoints in reverse order (both
+  // as per-slot graphs, captured on first use)
+  w.recg.assign(w.rec.size(), nullptr);
+  w.adjg.assign(w.rec.size(), nullptr);
   for (int sg = nck - 1; sg >= 0; sg--) {
     const int n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
     load_state(c, ck[sg]);
     for (int m = 0; m < len; m++) {
-      save_state(c, seg[m]);
-      if (m < len - 1) {
-        k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
-        CK(cudaGraphLaunch(c->gexec, s));
+      if (!w.recg[m]) {
+        const Rec* r = &w.rec[m];
+        rc = capture_graph(c, [r](harm_ctx* t) { return enqueue_step(t, nullptr, r); }, &w.recg[m]);
+        if (rc != HARM_OK) return rc;
       }
-    }
-    for (int m = len - 1; m >= 0; m--) {
-      double dtn;
-      CK(cudaMemcpyAsync(&dtn, w.dts + n0 + m, sizeof(double), cudaMemcpyDeviceToHost, s));
-      load_state(c, seg[m]);
       k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
-      if ((rc = enqueue_step(c, nullptr, &w.rec)) != HARM_OK) return rc;
-      CK(cudaStreamSynchronize(s));
-      adjoint_step(c, w, dtn, w_mass, w_em);
+      CK(cudaGraphLaunch(w.recg[m], s));
+    }
+    // the segment's last state, where its last step's adjoint reads it
+    CK(cudaMemcpyAsync(w.pnext[len - 1], c->d_p, P, cudaMemcpyDeviceToDevice, s));
+    for (int m = len - 1; m >= 0; m--) {
+      if (!w.adjg[m]) {
+        const Rec* r = &w.rec[m];
+        const double* po = w.pnext[m];
+        AdjWork* wp = &w;
+        rc = capture_graph(c, [=](harm_ctx* t) {
+          adjoint_step(t, *wp, *r, po, w_mass, w_em);
+          return HARM_OK;
+        }, &w.adjg[m]);
+        if (rc != HARM_OK) return rc;
+      }
+      k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
+      CK(cudaGraphLaunch(w.adjg[m], s));
     }
   }
   // through the input's bound: ghost adjoints onto the active zones

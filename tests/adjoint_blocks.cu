@@ -234,15 +234,14 @@ double ab_check_recon(int para, const double* y, const double* v, double lam_l, 
   return rel(fd, an);
 }
 
-// J_U^T x = b through primtoU_jacobian/solve_transpose8, checked as
-// <x, dU/dp v> = <b, v> with dU/dp v from finite differences of primtoU
+// J_U^T x = b through ift_solve, checked as <x, dU/dp v> = <b, v> with
+// dU/dp v from finite differences of primtoU
 double ab_check_ift(const double* p, const double* v, const double* b, const double* gcov16, const double* gcon16,
                     double gdet, double gam, double h)
 {
   const Geo<double> g = geo_of(gcov16, gcon16, gdet);
-  double J[NPR][NPR], x[NPR];
-  primtoU_jacobian(p, g, gam, J);
-  if (solve_transpose8(J, b, x)) return -1.;
+  double x[NPR];
+  if (ift_solve(p, g, gam, b, x)) return -1.;
   double pp[NPR], pm[NPR], Up[NPR], Um[NPR];
   for (int k = 0; k < NPR; k++) {
     pp[k] = p[k] + h * v[k];
@@ -270,10 +269,10 @@ void ab_primtoU(const double* p, const double* gcov16, const double* gcon16, dou
   state_of(p, g, q);
   flux_of<double, false>(p, q, 0, g, gam, U);
   if (J64) {
-    double J[NPR][NPR];
-    primtoU_jacobian(p, g, gam, J);
+    double J[5][NPR];
+    primtoU_jacobian5(p, g, gam, J);
     for (int r = 0; r < NPR; r++)
-      for (int c = 0; c < NPR; c++) J64[r * NPR + c] = J[r][c];
+      for (int c = 0; c < NPR; c++) J64[r * NPR + c] = (r < 5) ? J[r][c] : ((r == c) ? g.g : 0.);
   }
 }
 
