@@ -9,9 +9,10 @@
 // bound), k_adj_fixup, k_adj_poledeath + k_adj_ghosts (first bound),
 // k_adj_update (floors, limit, inverse function theorem on the con-to-prim
 // Jacobian, U(pi)), k_adj_source (geometric source), k_adj_corner (flux-CT
-// EMFs), k_adj_faces (face
-// fluxes and reconstructions, scattered onto pb with atomics).  All
-// adjoint arrays are planes in the step's layout, ghost zones included.
+// EMFs), then per direction k_adj_faces (face fluxes -> interface-state
+// adjoints) and k_adj_recon (reconstructions, scattered onto pb with
+// atomics).  All adjoint arrays are planes in the step's layout, ghost zones
+// included.
 #include <cuda_runtime.h>
 
 #include "harm_adjoint.cuh"
@@ -322,10 +323,12 @@ __global__ void k_adj_corner(StepArgs a, const double* __restrict__ lam_dU, doub
 
 // One face direction: the face-flux adjoint (from lam_dU of the two zones,
 // the EMF adjoints of its corners, and a seed seed_fac dt on the x1 mass flux
-// at i = 0), fix_flux's zeroed components, then the face and the two
-// reconstructions, scattered onto lam_b at the stencil zones.
+// at i = 0), fix_flux's zeroed components, then the face itself: sl, sr (8
+// planes each, indexed by the face) get the adjoints of its left and right
+// interface states, zero where the face carries none.  k_adj_recon takes
+// them through the reconstructions.
 __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const double* __restrict__ lam_dU,
-                            const double* __restrict__ lam_e, double* lam_b, int dir, double seed_fac)
+                            const double* __restrict__ lam_e, double* sl, double* sr, int dir, double seed_fac)
 {
   const double seed_mdot = seed_fac * a.sc->dt;
   const int i = blockIdx.x * blockDim.x + threadIdx.x - (dir == 2 ? 1 : 0);
@@ -370,12 +373,22 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
   }
   bool any = false;
   for (int k = 0; k < NPR; k++) any |= (Fb[k] != 0.);
-  if (!any) return;
+  double plb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.}, prb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  auto store = [&]() {
+    for (int k = 0; k < NPR; k++) {
+      sl[k * pl + z] = plb[k];
+      sr[k * pl + z] = prb[k];
+    }
+  };
+  if (!any) {
+    store();
+    return;
+  }
   // the two interface states: right state of zone (i-di, j-dj), left of (i, j)
   const int para = (a.pp.lim == 4);
   const long long s = (dir == 1) ? 1LL : (long long)a.gr.pitch;
   const long long zl = z - s;
-  double pls[NPR], prs[NPR], cl[NPR][5], cr[NPR][5];
+  double pls[NPR], prs[NPR];
   for (int k = 0; k < NPR; k++) {
     double yl[5], yr[5];
     for (int m = 0; m < 5; m++) {
@@ -384,9 +397,6 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
       yl[m] = in ? pb[k * pl + zl + o] : 0.;
       yr[m] = in ? pb[k * pl + z + o] : 0.;
     }
-    double tl[5], tr[5];
-    recon_rows(para, yl, tl, cr[k]);  // zone i-1: its right state is the face's left
-    recon_rows(para, yr, cl[k], tr);  // zone i: its left state is the face's right
     double lo, ro;
     if (para) {
       para4(yl[0], yl[1], yl[2], yl[3], yl[4], lo, ro);
@@ -399,8 +409,6 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
       dq = mc_slope(yr[1], yr[2], yr[3]);
       prs[k] = yr[2] - 0.5 * dq;
     }
-    (void)tl;
-    (void)tr;
   }
   Geo<double> g;
   load_geo(a, dir == 1 ? FACE1 : FACE2, z, g);
@@ -411,14 +419,42 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
       if ((i == 0 && Fo[RHO] > 0) || (i == n1 && Fo[RHO] < 0)) Fb[RHO] = 0.;
     }
   }
-  double plb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.}, prb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
-  if (adj_face_flux(pls, prs, g, dir, a.pp.gam, a.pp.gammamax, a.pp.fluxmethod, Fb, plb, prb)) return;
+  if (adj_face_flux(pls, prs, g, dir, a.pp.gam, a.pp.gammamax, a.pp.fluxmethod, Fb, plb, prb))
+    for (int k = 0; k < NPR; k++) plb[k] = prb[k] = 0.;
+  store();
+}
+
+// The reconstructions of one direction backwards: zone (i, j), i in
+// [-1, N1], j in [-1, N2], has its left state on face (i, j) (that face's
+// right state, adjoint sr) and its right state on the next face (that
+// face's left state, adjoint sl); its MC/PARA4 rows (both states from one
+// evaluation) scatter them onto lam_b at the stencil zones.
+__global__ void k_adj_recon(StepArgs a, const double* __restrict__ pb, const double* __restrict__ sl,
+                            const double* __restrict__ sr, double* lam_b, int dir)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (i > n1 || j > n2) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  const long long s = (dir == 1) ? 1LL : (long long)a.gr.pitch;
+  // faces of this direction: x1 i in [0, N1], j in [-1, N2]; x2 j in [0, N2], i in [-1, N1]
+  const int f0 = (dir == 1) ? i : j, nf = (dir == 1) ? n1 : n2;
+  const bool has_l = (f0 >= 0 && f0 <= nf), has_r = (f0 + 1 >= 0 && f0 + 1 <= nf);
+  const int para = (a.pp.lim == 4);
   for (int k = 0; k < NPR; k++) {
+    const double ll = has_l ? sr[k * pl + z] : 0., lr = has_r ? sl[k * pl + z + s] : 0.;
+    if (ll == 0. && lr == 0.) continue;
+    double y[5];
     for (int m = 0; m < 5; m++) {
-      const long long o = (long long)(m - 2) * s;
-      const double vl = cr[k][m] * plb[k], vr = cl[k][m] * prb[k];
-      if (vl != 0.) atomicAdd(&lam_b[k * pl + zl + o], vl);
-      if (vr != 0.) atomicAdd(&lam_b[k * pl + z + o], vr);
+      const bool in = para || (m >= 1 && m <= 3);
+      y[m] = in ? pb[k * pl + z + (long long)(m - 2) * s] : 0.;
+    }
+    double cl[5], cr[5];
+    recon_rows(para, y, cl, cr);
+    for (int m = 0; m < 5; m++) {
+      const double v = cl[m] * ll + cr[m] * lr;
+      if (v != 0.) atomicAdd(&lam_b[k * pl + z + (long long)(m - 2) * s], v);
     }
   }
 }

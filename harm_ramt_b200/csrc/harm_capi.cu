@@ -44,8 +44,9 @@ __global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, 
                              double cfac, double* lam_pi, double* lam_dU);
 __global__ void k_adj_source(StepArgs a, const double* pb, const double* lam_dU, double* lam_b);
 __global__ void k_adj_corner(StepArgs a, const double* lam_dU, double* lam_e);
-__global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* lam_b,
-                            int dir, double seed_fac);
+__global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* sl,
+                            double* sr, int dir, double seed_fac);
+__global__ void k_adj_recon(StepArgs a, const double* pb, const double* sl, const double* sr, double* lam_b, int dir);
 __global__ void k_set_dt(StepArgs a, const double* dts, int k);
 __global__ void k_get_dt(StepArgs a, double* dts, int k);
 __global__ void k_axpy(double* y, const double* x, long long n);
@@ -813,7 +814,7 @@ struct AdjWork {
   std::vector<double*> pnext;  // the state after each slot's step (the next slot's pn; an extra one at the end)
   std::vector<cudaGraphExec_t> recg;  // the recording step of each slot, captured
   std::vector<cudaGraphExec_t> adjg;  // the adjoint step of each slot, captured
-  double *La, *Lc, *Lb, *Lsnap, *LdU, *Le, *dts, *dot;
+  double *La, *Lc, *Lb, *Lsnap, *LdU, *Le, *Sr, *dts, *dot;
   bool ok = true;
   void* get(size_t bytes)
   {
@@ -874,6 +875,7 @@ int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps, int nslots)
   w.Lb = (double*)w.get(P);
   w.Lsnap = (double*)w.get(P);
   w.LdU = (double*)w.get(P);
+  w.Sr = (double*)w.get(P);
   w.Le = (double*)w.get(pl * sizeof(double));
   w.dts = (double*)w.get((size_t)nsteps * sizeof(double));
   w.dot = (double*)w.get(dot_blocks(c) * sizeof(double));
@@ -915,8 +917,11 @@ void adjoint_substep(harm_ctx* c, AdjWork& w, const Rec& r, int sub, double* lam
   k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], pi, cfac, lam_pi_acc, w.LdU);
   k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, out);
   k_adj_corner<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a, w.LdU, w.Le);
-  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, out, 1, seed_fac);
-  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, out, 2, 0.);
+  // the face-state adjoints go to Lsnap (free after the update) and Sr
+  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, 1, seed_fac);
+  k_adj_recon<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out, 1);
+  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, 2, 0.);
+  k_adj_recon<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out, 2);
 }
 
 // step n's adjoint from its record r and its output state pout (p^{n+1}),
