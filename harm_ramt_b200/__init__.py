@@ -93,7 +93,8 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_torus_default_params", "harm_torus_geometry", "harm_torus_init", "harm_profile_step",
            "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
            "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
-           "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt"]
+           "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt",
+           "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint"]
 
 
 def load_library(path=None):
@@ -131,6 +132,9 @@ def load_library(path=None):
     lib.harm_torus_default_params.restype = None
     lib.harm_torus_geometry.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp, dp, dp]
     lib.harm_torus_init.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
+    lib.harm_torus_init_vpot.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp, dp, dp]
+    lib.harm_torus_vpot_to_field.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
+    lib.harm_torus_vpot_adjoint.argtypes = [ctypes.POINTER(_TorusParams), dp, dp, dp, dp]
     lib.harm_profile_step.argtypes = [vp, dp, ip, ctypes.c_int]
     lib.harm_get_horizon.argtypes = [vp, dp]
     lib.harm_get_currents.argtypes = [vp, dp, dp, dp]
@@ -202,6 +206,42 @@ def torus_init(params, geom):
     _check(lib.harm_torus_init(ctypes.byref(params), _dp(geom["gcov"]), _dp(geom["gcon"]), _dp(geom["gdet"]),
                                _dp(p)), "harm_torus_init")
     return p
+
+
+def torus_init_vpot(params, geom):
+    """torus_init() with the corner vector potential A_phi [n1+1, n2+1] and
+    the two field normalisation factors: (prims, A, norm)."""
+    lib = load_library()
+    n1m, n2m = params.n1 + 2 * NG, params.n2 + 2 * NG
+    p = np.zeros((n1m, n2m, NPR))
+    A = np.zeros((params.n1 + 1, params.n2 + 1))
+    norm = np.zeros(2)
+    _check(lib.harm_torus_init_vpot(ctypes.byref(params), _dp(geom["gcov"]), _dp(geom["gcon"]), _dp(geom["gdet"]),
+                                    _dp(p), _dp(A), _dp(norm)), "harm_torus_init_vpot")
+    return p, A, norm
+
+
+def vpot_to_field(params, geom, A, norm, prims):
+    """A copy of prims whose active B1, B2 come from the vector potential A
+    (normalised by the fixed factors norm)."""
+    lib = load_library()
+    p = np.ascontiguousarray(prims, dtype=np.float64).copy()
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    norm = np.ascontiguousarray(norm, dtype=np.float64)
+    _check(lib.harm_torus_vpot_to_field(ctypes.byref(params), _dp(geom["gdet"]), _dp(A), _dp(norm), _dp(p)),
+           "harm_torus_vpot_to_field")
+    return p
+
+
+def vpot_adjoint(params, geom, grad, norm):
+    """dJ/dA [n1+1, n2+1] from dJ/dprims (e.g. HarmGPU.adjoint's gradient)."""
+    lib = load_library()
+    g = np.ascontiguousarray(grad, dtype=np.float64)
+    norm = np.ascontiguousarray(norm, dtype=np.float64)
+    gA = np.zeros((params.n1 + 1, params.n2 + 1))
+    _check(lib.harm_torus_vpot_adjoint(ctypes.byref(params), _dp(geom["gdet"]), _dp(g), _dp(norm), _dp(gA)),
+           "harm_torus_vpot_adjoint")
+    return gA
 
 
 # ----------------------------------------------------------------- device

@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/harm_b200.h"
@@ -445,10 +446,13 @@ int harm_torus_dump_coords(const harm_torus_params* P, harm_dump_header* hdr, do
   return HARM_OK;
 }
 
-int harm_torus_init(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet, double* prims)
+}  // extern "C"
+
+namespace {
+
+// MKS defcoord 0 coordinates of the torus grid
+Coords torus_coords(const harm_torus_params* P)
 {
-  if (!P || !gcov || !gcon || !gdet || !prims) return HARM_EINVAL;
-  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG, n1m = n1 + 2 * NG;
   Coords c;
   c.a = P->a;
   c.R0 = 0.0;
@@ -458,8 +462,19 @@ int harm_torus_init(const harm_torus_params* P, const double* gcov, const double
   c.hslope = P->hslope;
   c.startx1 = log(c.Rin - c.R0);
   c.startx2 = 0.;
-  c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / n1;
-  c.dx2 = 1. / n2;
+  c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / P->n1;
+  c.dx2 = 1. / P->n2;
+  return c;
+}
+
+// init() for the torus; A (may be NULL) receives the corner vector
+// potential, norm (may be NULL) the two field normalisation factors
+int torus_init_impl(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet,
+                    double* prims, double* A_out, double* norm_out)
+{
+  if (!P || !gcov || !gcon || !gdet || !prims) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG, n1m = n1 + 2 * NG;
+  const Coords c = torus_coords(P);
   const double a = c.a, gam = P->gam;
   auto Z = [&](int i, int j) { return (long long)(i + NG) * n2m + (j + NG); };
   auto geo = [&](int i, int j) {
@@ -684,6 +699,7 @@ int harm_torus_init(const harm_torus_params* P, const double* gcov, const double
       }
     const double beta_act = (gam - 1.) * umax / (0.5 * bsq_max);
     const double norm = sqrt(beta_act / P->beta);
+    if (norm_out) norm_out[pass] = norm;
     for (int i = 0; i < n1; i++)
       for (int j = 0; j < n2; j++) {
         PR(i, j)[B1] *= norm;
@@ -692,6 +708,69 @@ int harm_torus_init(const harm_torus_params* P, const double* gcov, const double
       }
   }
   fixup_all();
+  if (A_out) std::copy(A.begin(), A.end(), A_out);
+  return HARM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int harm_torus_init(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet, double* prims)
+{
+  return torus_init_impl(P, gcov, gcon, gdet, prims, nullptr, nullptr);
+}
+
+int harm_torus_init_vpot(const harm_torus_params* P, const double* gcov, const double* gcon, const double* gdet,
+                         double* prims, double* A, double* norm)
+{
+  if (!A || !norm) return HARM_EINVAL;
+  return torus_init_impl(P, gcov, gcon, gdet, prims, A, norm);
+}
+
+int harm_torus_vpot_to_field(const harm_torus_params* P, const double* gdet, const double* A, const double* norm,
+                             double* prims)
+{
+  if (!P || !gdet || !A || !norm || !prims) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG;
+  const Coords c = torus_coords(P);
+  auto AA = [&](int i, int j) { return A[(size_t)i * (n2 + 1) + j]; };
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      const long long z = (long long)(i + NG) * n2m + (j + NG);
+      const double g = gdet[z * 4 + CENT];
+      double* pr = prims + z * 8;
+      // vpot2field (initbase.c:565-618), then the two normalisations
+      pr[B1] = (-AA(i, j) + AA(i, j + 1) - AA(i + 1, j) + AA(i + 1, j + 1)) / (2. * c.dx2 * g);
+      pr[B2] = -(-AA(i, j) - AA(i, j + 1) + AA(i + 1, j) + AA(i + 1, j + 1)) / (2. * c.dx1 * g);
+      for (int pass = 0; pass < 2; pass++) {
+        pr[B1] *= norm[pass];
+        pr[B2] *= norm[pass];
+      }
+    }
+  return HARM_OK;
+}
+
+int harm_torus_vpot_adjoint(const harm_torus_params* P, const double* gdet, const double* grad_prims,
+                            const double* norm, double* grad_A)
+{
+  if (!P || !gdet || !grad_prims || !norm || !grad_A) return HARM_EINVAL;
+  const int n1 = P->n1, n2 = P->n2, n2m = n2 + 2 * NG;
+  const Coords c = torus_coords(P);
+  const double s = norm[0] * norm[1];
+  for (size_t k = 0; k < (size_t)(n1 + 1) * (n2 + 1); k++) grad_A[k] = 0.;
+  auto GA = [&](int i, int j) -> double& { return grad_A[(size_t)i * (n2 + 1) + j]; };
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < n2; j++) {
+      const long long z = (long long)(i + NG) * n2m + (j + NG);
+      const double g = gdet[z * 4 + CENT];
+      const double c1 = grad_prims[z * 8 + B1] * s / (2. * c.dx2 * g);
+      const double c2 = grad_prims[z * 8 + B2] * s / (2. * c.dx1 * g);
+      GA(i, j) += -c1 + c2;
+      GA(i, j + 1) += c1 + c2;
+      GA(i + 1, j) += -c1 - c2;
+      GA(i + 1, j + 1) += c1 - c2;
+    }
   return HARM_OK;
 }
 

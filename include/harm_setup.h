@@ -51,6 +51,27 @@ int harm_torus_geometry(const harm_torus_params* p, double* gcov, double* gcon, 
 int harm_torus_init(const harm_torus_params* p, const double* gcov, const double* gcon, const double* gdet,
                     double* prims);
 
+/* harm_torus_init() that also returns the corner vector potential A_phi
+   (init_vpot, init.fishmon.c:236-268), [n1+1][n2+1] at corners (i, j) of
+   the active grid, and the two field normalisation factors norm[2]
+   (normalize_field, init.fishmon.c:310-375, applied twice). */
+int harm_torus_init_vpot(const harm_torus_params* p, const double* gcov, const double* gcon, const double* gdet,
+                         double* prims, double* A, double* norm);
+
+/* B1, B2 of the active zones from a corner vector potential: vpot2field
+   (initbase.c:565-618) then the normalisation by norm[0], norm[1] (the
+   factors harm_torus_init_vpot() returned, held fixed).  With the A and
+   norm of harm_torus_init_vpot() it reproduces the init's field exactly. */
+int harm_torus_vpot_to_field(const harm_torus_params* p, const double* gdet, const double* A, const double* norm,
+                             double* prims);
+
+/* The adjoint of harm_torus_vpot_to_field(): grad_A [n1+1][n2+1] from the
+   gradient grad_prims [n1m][n2m][8] of an objective with respect to the
+   primitives (its B1, B2 entries of the active zones), e.g. the gradient
+   harm_adjoint_run() returns with respect to the initial state. */
+int harm_torus_vpot_adjoint(const harm_torus_params* p, const double* gdet, const double* grad_prims,
+                            const double* norm, double* grad_A);
+
 /* The coordinate columns of the torus grid for harm_write_dump(): the dump
    header's plugin scalars (defcoord 0) and X1, X2, r, th at every zone
    centre, [n1m][n2m][4] (coord.c:920-938, bl_coord coord.c:334-453). */
