@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=64, help="tori in the batched-ensemble leg (0: skip it)")
     ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--ensemble-steps-per-launch", type=int, default=10)
+    ap.add_argument("--adjoint-n", type=int, default=256, help="grid of the adjoint leg (0: skip it)")
+    ap.add_argument("--adjoint-t", type=float, default=100.0,
+                    help="the adjoint leg runs as many steps as the forward run from init takes to this time")
+    ap.add_argument("--adjoint-ckpt", type=int, default=16)
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
@@ -316,6 +320,9 @@ def b200_arm(a):
     ens = None
     if a.ensemble > 0:
         ens = ensemble_leg(a, hb, stream, lim, flux, barrier, dist)
+    adj = None
+    if a.adjoint_n > 0:
+        adj = adjoint_leg(a, hb, dist)
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -340,13 +347,59 @@ def b200_arm(a):
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
-                "ensemble": ens,
+                "ensemble": ens, "adjoint": adj,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def adjoint_leg(a, hb, dist):
+    """The differentiated form on its configuration: the adjoint_n^2 torus
+    from init (MC + HLL, the seeded 4% u perturbation), as many steps as a
+    run from init takes to t = adjoint_t (so that the torus and the horizon
+    are causally connected), a checkpoint every adjoint_ckpt steps, then
+    the adjoint back to the initial state (harm_adjoint_run) for J = sum_n
+    dt_n (horizon mass flux + horizon EM energy flux).  Reports device times
+    of the forward and the backward pass (max over ranks) and the gradient's
+    size with respect to the initial A_phi and u.  One untimed short call
+    first loads the kernels."""
+    n, C = a.adjoint_n, a.adjoint_ckpt
+    par = hb.torus_params(n, n)
+    geom = hb.torus_geometry(par)
+    p0, A, norm = hb.torus_init_vpot(par, geom)
+
+    def ctx():
+        h = hb.HarmGPU(n, n, geom["dx1"], geom["dx2"], lim=hb.LIM_MC, fluxmethod=hb.FLUX_HLL, gam=par.gam,
+                       gammamax=par.gammamax)
+        h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
+        h.set_prims(p0)
+        h.set_time(0.0, 1e-5, 0)
+        return h
+
+    h = ctx()
+    K = int(h.run_to(a.adjoint_t)["realnstep"])
+    h.close()
+    h = ctx()
+    h.adjoint(C, C, 1.0, 1.0, None)
+    h.close()
+    h = ctx()
+    J, grad, dts, ms = h.adjoint(K, C, 1.0, 1.0, None)
+    h.close()
+    fwd, bwd = max_over_ranks(ms[0], dist, "cuda"), max_over_ranks(ms[1], dist, "cuda")
+    gA = hb.vpot_adjoint(par, geom, grad, norm)
+    return {"workload": f"{n}x{n} Fishbone-Moncrief torus from init (seeded 4% u perturbation), MC + HLL, FP64",
+            "steps": K, "checkpoint_every": C, "t_end": float(dts.sum()),
+            "grad_A_phi_l2": float((gA ** 2).sum() ** 0.5), "grad_u_l2": float((grad[..., 1] ** 2).sum() ** 0.5),
+            "objective": "sum_n dt_n (horizon mass flux + horizon EM energy flux)", "J": J,
+            "forward_ms": fwd, "backward_ms": bwd, "forward_ms_per_step": fwd / K, "backward_ms_per_step": bwd / K,
+            "backward_over_forward": bwd / fwd,
+            "grad_A_phi_max": float(abs(gA).max()), "grad_u_max": float(abs(grad[..., 1]).max()),
+            "dJ_dlnu_max": float(abs(grad[..., 1] * p0[..., 1]).max()),
+            "dJ_dA_phi_times_A_max": float(abs(gA).max() * abs(A).max()),
+            "note": "backward = segment replays with recording + adjoint kernels, per-slot graphs captured in the call"}
 
 
 def ensemble_leg(a, hb, stream, lim, flux, barrier, dist):

@@ -429,6 +429,14 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
 // right state, adjoint sr) and its right state on the next face (that
 // face's left state, adjoint sl); its MC/PARA4 rows (both states from one
 // evaluation) scatter them onto lam_b at the stencil zones.
+// A field component whose whole stencil lies below B_NOISE sqrt(rho) of
+// the zone (b^2/rho < 1e-20: round-off left where no field has arrived)
+// takes the rows of a tie (each state = the zone's value).  There the
+// limiter's branch is set by round-off, the exact derivative holds only for
+// perturbations below that level, and its transpose over many steps grows
+// without bound; any resolvable perturbation sees the tie's rows.
+constexpr double B_NOISE = 1e-10;
+
 __global__ void k_adj_recon(StepArgs a, const double* __restrict__ pb, const double* __restrict__ sl,
                             const double* __restrict__ sr, double* lam_b, int dir)
 {
@@ -442,16 +450,22 @@ __global__ void k_adj_recon(StepArgs a, const double* __restrict__ pb, const dou
   const int f0 = (dir == 1) ? i : j, nf = (dir == 1) ? n1 : n2;
   const bool has_l = (f0 >= 0 && f0 <= nf), has_r = (f0 + 1 >= 0 && f0 + 1 <= nf);
   const int para = (a.pp.lim == 4);
+  const double bnoise = B_NOISE * sqrt(fmax(pb[RHO * pl + z], 0.));
   for (int k = 0; k < NPR; k++) {
     const double ll = has_l ? sr[k * pl + z] : 0., lr = has_r ? sl[k * pl + z + s] : 0.;
     if (ll == 0. && lr == 0.) continue;
-    double y[5];
+    double y[5], ymax = 0.;
     for (int m = 0; m < 5; m++) {
       const bool in = para || (m >= 1 && m <= 3);
       y[m] = in ? pb[k * pl + z + (long long)(m - 2) * s] : 0.;
+      ymax = fmax(ymax, fabs(y[m]));
     }
     double cl[5], cr[5];
-    recon_rows(para, y, cl, cr);
+    if (k >= B1 && ymax < bnoise) {
+      for (int m = 0; m < 5; m++) cl[m] = cr[m] = (m == 2) ? 1. : 0.;
+    } else {
+      recon_rows(para, y, cl, cr);
+    }
     for (int m = 0; m < 5; m++) {
       const double v = cl[m] * ll + cr[m] * lr;
       if (v != 0.) atomicAdd(&lam_b[k * pl + z + (long long)(m - 2) * s], v);
