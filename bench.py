@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--adjoint-t", type=float, default=100.0,
                     help="the adjoint leg runs as many steps as the forward run from init takes to this time")
     ap.add_argument("--adjoint-ckpt", type=int, default=16)
+    ap.add_argument("--adjoint-steps", type=int, default=0,
+                    help="if > 0, the adjoint leg runs this many steps instead of running to --adjoint-t")
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
@@ -379,9 +381,12 @@ def adjoint_leg(a, hb, dist):
         h.set_time(0.0, 1e-5, 0)
         return h
 
-    h = ctx()
-    K = int(h.run_to(a.adjoint_t)["realnstep"])
-    h.close()
+    if a.adjoint_steps > 0:
+        K = a.adjoint_steps
+    else:
+        h = ctx()
+        K = int(h.run_to(a.adjoint_t)["realnstep"])
+        h.close()
     h = ctx()
     h.adjoint(C, C, 1.0, 1.0, None)
     h.close()
@@ -549,7 +554,7 @@ KERNEL_BYTES = {
 }
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
 # at 512^2 (profiles/k_*_torus512_fp64_para_hll.md), scaled by zone count
-TRAFFIC_512 = {"k_flux": 109.3e6, "k_update": 194.1e6}
+TRAFFIC_512 = {"k_flux": 113.8e6, "k_update": 212.2e6}
 
 
 def main():
