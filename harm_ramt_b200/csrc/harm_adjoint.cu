@@ -8,7 +8,7 @@
 // harm_capi.cu, adjoint_substep): k_adj_poledeath + k_adj_ghosts (second
 // bound), k_adj_fixup, k_adj_poledeath + k_adj_ghosts (first bound),
 // k_adj_update (floors, limit, inverse function theorem on the con-to-prim
-// Jacobian, U(pi)), k_adj_source (geometric source), k_adj_corner (flux-CT
+// Jacobian), k_adj_upi (U(pi)), k_adj_source (geometric source), k_adj_corner (flux-CT
 // EMFs), then per direction k_adj_faces (face fluxes -> interface-state
 // adjoints) and k_adj_recon (reconstructions, scattered onto pb with
 // atomics).  All adjoint arrays are planes in the step's layout, ghost zones
@@ -223,17 +223,17 @@ __global__ void k_adj_fixup(StepArgs a, const double* __restrict__ lam_in, doubl
     if (lp[k] != 0.) atomicAdd(&lam_snap[k * pl + z], lp[k]);
 }
 
-// The zone update: lam (adjoint of the update's output) -> lam_pi (+= own
-// zone, from U(pi)), lam_dU (= c dt Ubar, for the fluxes and the source;
-// c = cfac, dt the step's a.sc->dt).
+// The zone update's con-to-prim: lam (adjoint of the update's output) ->
+// ubar (Ubar, the adjoint of the updated conserved vector) and lam_dU (=
+// c dt Ubar, for the fluxes and the source; c = cfac, dt the step's
+// a.sc->dt).
 // pinv: the inverted primitives before floors; flaginv: the inversion's
 // pflag.  The geometric source's adjoint is k_adj_source's: built into this
 // kernel (after the con-to-prim Jacobian), sm_100a code of nvcc 12.9 gave
 // source adjoints that differ from the same function's host build and from
 // finite differences, at any ptxas optimisation level.
 __global__ void k_adj_update(StepArgs a, const double* __restrict__ lam, const double* __restrict__ pinv,
-                             const int* __restrict__ flaginv, const double* __restrict__ pi, double cfac,
-                             double* lam_pi, double* lam_dU)
+                             const int* __restrict__ flaginv, double cfac, double* ubar, double* lam_dU)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (!active(a, i, j)) return;
@@ -264,20 +264,33 @@ __global__ void k_adj_update(StepArgs a, const double* __restrict__ lam, const d
     if (ift_solve(p1, g, gam, l1, Ub))
       for (int k = 0; k < NPR; k++) Ub[k] = 0.;
   }
-  // Uf = U(pi) + cdt (dUr + dUg)
-  {
-    double p[NPR];
-    load_prims(pi, pl, z, p);
-    State<double> q;
-    state_of(p, g, q);
-    StateAdj qb;
-    qb.zero();
-    double lpi[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
-    adj_flux(p, q, 0, g, gam, Ub, qb, lpi);
-    adj_state(p, g, q, qb, lpi);
-    for (int k = 0; k < NPR; k++) lam_pi[k * pl + z] += lpi[k];
+  for (int k = 0; k < NPR; k++) {
+    ubar[k * pl + z] = Ub[k];
+    lam_dU[k * pl + z] = cdt * Ub[k];
   }
-  for (int k = 0; k < NPR; k++) lam_dU[k * pl + z] = cdt * Ub[k];
+}
+
+// Uf = U(pi) + c dt (dUr + dUg): the U(pi) part, lam_pi += (dU/dp at pi)^T
+// ubar (a kernel of its own: with the implicit-function step in the same
+// kernel both ran at two blocks per SM)
+__global__ void k_adj_upi(StepArgs a, const double* __restrict__ ubar, const double* __restrict__ pi, double* lam_pi)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (!active(a, i, j)) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  double Ub[NPR], p[NPR];
+  load_prims(ubar, pl, z, Ub);
+  load_prims(pi, pl, z, p);
+  State<double> q;
+  state_of(p, g, q);
+  StateAdj qb;
+  qb.zero();
+  double lpi[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  adj_flux(p, q, 0, g, a.pp.gam, Ub, qb, lpi);
+  adj_state(p, g, q, qb, lpi);
+  for (int k = 0; k < NPR; k++) lam_pi[k * pl + z] += lpi[k];
 }
 
 // The geometric source dUg[UU+l] = g sum_jj sum_k T^jj_k Gamma^k_{l jj} at

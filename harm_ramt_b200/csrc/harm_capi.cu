@@ -40,8 +40,9 @@ __global__ void k_adj_poledeath(StepArgs a, double* lam);
 __global__ void k_adj_ghosts(StepArgs a, double* lam, const double* src);
 __global__ void k_adj_fixup(StepArgs a, const double* lam_in, double* lam_snap, const double* snap, const int* flag,
                             const unsigned char* fixset);
-__global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, const int* flaginv, const double* pi,
-                             double cfac, double* lam_pi, double* lam_dU);
+__global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, const int* flaginv, double cfac,
+                             double* ubar, double* lam_dU);
+__global__ void k_adj_upi(StepArgs a, const double* ubar, const double* pi, double* lam_pi);
 __global__ void k_adj_source(StepArgs a, const double* pb, const double* lam_dU, double* lam_b);
 __global__ void k_adj_corner(StepArgs a, const double* lam_dU, double* lam_e);
 __global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* sl,
@@ -914,7 +915,8 @@ void adjoint_substep(harm_ctx* c, AdjWork& w, const Rec& r, int sub, double* lam
   k_adj_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, w.Lsnap);
   k_adj_ghosts<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, w.Lsnap, r.upd[sub]);
   cudaMemsetAsync(out, 0, P, s);
-  k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], pi, cfac, lam_pi_acc, w.LdU);
+  k_adj_update<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Lsnap, r.pinv[sub], r.flaginv[sub], cfac, w.Sr, w.LdU);
+  k_adj_upi<<<grid2(n1, n2, b), b, 0, s>>>(a, w.Sr, pi, lam_pi_acc);
   k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, out);
   k_adj_corner<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a, w.LdU, w.Le);
   // the face-state adjoints go to Lsnap (free after the update) and Sr
