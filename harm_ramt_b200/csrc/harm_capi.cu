@@ -203,7 +203,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     const int mixed = c->cfg.precision == HARM_PREC_MIXED;
     const int ffde = c->cfg.eom == HARM_EOM_FFDE;
     const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, grid2(n1 + 2, n2 + 2, fb), fb, s, a, pb);
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2), fb, s, a, pb);
     T.mark(s, KC_FLUX);
     launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
@@ -308,7 +308,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   c->gr.plane = (long long)c->gr.pitch * c->gr.rows;
   const size_t pd = (size_t)c->gr.plane * sizeof(double);
   const dim3 b(32, 4);
-  dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, dim3(32, FLUX_BY));
+  dim3 gf = flux_grid(cfg->n1, cfg->n2);
   c->nblocks_flux = gf.x * gf.y;
   c->tile_update = dim3(32, 4);
   c->tile_small = dim3(32, 4);
@@ -1286,7 +1286,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.gr.rows = c.n2m;
   c.gr.plane = (long long)c.gr.pitch * c.gr.rows;
   const dim3 b(32, 4);
-  const dim3 gf = grid2(cfg->n1 + 2, cfg->n2 + 2, dim3(32, FLUX_BY));
+  const dim3 gf = flux_grid(cfg->n1, cfg->n2);
   c.nblocks_flux = gf.x * gf.y;
   c.tile_update = dim3(32, 4);
   c.tile_small = dim3(32, 4);

@@ -117,8 +117,11 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
 
-// k_flux blocks: 32 zones along x1 (one warp) x FLUX_BY rows
-constexpr int FLUX_BY = 4;
+// k_flux blocks: 32 zones along x1 (one warp) x FLUX_BY rows.  Neighbouring
+// blocks overlap by one zone along x1, so that each covers FLUX_BX x1 faces
+// without recomputing a neighbour's interface state.
+constexpr int FLUX_BY = 4, FLUX_BX = 31;
+inline dim3 flux_grid(int n1, int n2) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + FLUX_BY - 1) / FLUX_BY); }
 
 // plane offsets of the currents block
 constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 21, CUR_NPLANES = 25;

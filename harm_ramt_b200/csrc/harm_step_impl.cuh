@@ -114,7 +114,11 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // flux clamp only where that end is OUTFLOW, i.e. for the torus).  Blocks are
 // 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
 // states once: the x1 neighbour's right state arrives by warp shuffle and
-// the x2 neighbour's through shared memory (the first lane/row recomputes).
+// the x2 neighbour's through shared memory (the first row recomputes).
+// Lane 0's zone is also the previous block's lane 31 (blocks step by
+// FLUX_BX = 31 along x1): lane 0 only lends its right state, and its faces
+// are the previous block's (block 0's lane 0 is zone -1, which has no x1
+// face but an x2 face).
 // FP64: at most 128 registers (4 blocks per SM); the register-light FP32
 // faces of the mixed form are left unconstrained
 template <typename T, bool PARA, bool FFDE>
@@ -123,10 +127,11 @@ __global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 4 : 1) k_flux
   __shared__ double sh[2][32];
   __shared__ T shr[NPR][FLUX_BY][32];
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i = blockIdx.x * 32 + tx - 1;
+  const int i = blockIdx.x * FLUX_BX + tx - 1;
   const int j = blockIdx.y * FLUX_BY + ty - 1;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   const bool in = (i <= n1) && (j <= n2);
+  const bool own = (tx > 0) || (blockIdx.x == 0);  // lane 0 of a later block repeats a zone
   // threads past the grid work on a clamped (valid) zone; their results are unused
   const int ic = (i <= n1) ? i : n1, jc = (j <= n2) ? j : n2;
   double dt1 = 1.e9, dt2 = 1.e9;
@@ -140,11 +145,7 @@ __global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 4 : 1) k_flux
   zone_states<T, PARA>(a, pb, ic, jc, 1, L, R);
 #pragma unroll
   for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
-  if (tx == 0 && ic >= 0) {
-    T Lm[NPR];
-    zone_states<T, PARA>(a, pb, ic - 1, jc, 1, Lm, pl);
-  }
-  if (in && i >= 0) {
+  if (in && i >= 0 && tx > 0) {
     face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij);
     dt1 = (dtij < dt1) ? dtij : dt1;
     if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 4 : 1) k_flux
     T Lm[NPR];
     zone_states<T, PARA>(a, pb, ic, jc - 1, 2, Lm, pl);
   }
-  if (in && j >= 0) {
+  if (in && j >= 0 && own) {
     face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
     dt2 = (dtij < dt2) ? dtij : dt2;
     const bool polar = (j == 0 || j == n2) && (i < n1);
