@@ -25,7 +25,7 @@ namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
-__global__ void k_gammacheck(StepArgs a, const double* pv);
+__global__ void k_gammacheck(StepArgs a, double* pv, int poledeath);
 __global__ void k_checksol(StepArgs a, const double* pv, int round);
 __global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
 __global__ void k_fixup_compute(StepArgs a, const double* pv);
@@ -215,16 +215,20 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     }
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
-    if (poledeath) {
-      k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
-      T.mark(s, KC_POLE);
-    }
-    if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
     // force-free: no b^2 flags (so no check-solution votes) and no
     // fixup_utoprim (fixup.c:542); the second bound would repeat the first
-    if (ffde) continue;
-    k_gammacheck<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pf);
+    if (ffde) {
+      if (poledeath) {
+        k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
+        T.mark(s, KC_POLE);
+      }
+      if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
+      continue;
+    }
+    // the POLEDEATH zeroing after this bound is applied inside k_gammacheck
+    k_gammacheck<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pf, poledeath ? 1 : 0);
     T.mark(s, KC_GCHECK);
+    if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
     for (int r = 0; r < CHK_ROUNDS; r++) {
       k_checksol<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, r);
       T.mark(s, KC_CHECKSOL);

@@ -223,13 +223,21 @@ __global__ void k_poledeath(StepArgs a, double* pv)
 
 // ---------------------------------------------------------------- check solution
 // fixup_checksolution, fixup.c:388-488.  gammacheck first (DQZLOOP range).
-__global__ void k_gammacheck(StepArgs a, const double* __restrict__ pv)
+// With poledeath set, each thread of the first or last active row first
+// applies the POLEDEATH zeroing of k_poledeath to its own zone (the bound
+// before this kernel has read those rows already; this kernel reads only
+// its own zone).
+__global__ void k_gammacheck(StepArgs a, double* __restrict__ pv, int poledeath)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 8 && threadIdx.y == 0) a.sc->chk_changed[threadIdx.x] = 0;
   if (i > a.gr.n1 || j > a.gr.n2) return;
   const long long z = a.gr.at(i, j);
+  if (poledeath && i >= 0 && i < a.gr.n1 && (j == 0 || j == a.gr.n2 - 1)) {
+    pv[U2 * a.gr.plane + z] *= 0.;
+    pv[B2 * a.gr.plane + z] *= 0.;
+  }
   if (a.bsqf[z] == 0 || a.pflag[z] != 0) return;
   double pr[NPR];
 #pragma unroll
@@ -442,6 +450,31 @@ __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd)
 __global__ void k_dt_finalize(StepArgs a)
 {
   __shared__ double sh[2][32];
+  __shared__ double acc[4];
+  __shared__ double buf[4][256];
+  // the horizon sums of k_horizon's per-j terms, in j order (diag.c:576-833):
+  // the block stages 256 j at a time in shared memory, four threads add
+  if (threadIdx.x < 4) acc[threadIdx.x] = 0.;
+  for (int j0 = 0; j0 < a.gr.n2; j0 += 256) {
+    const int m = (a.gr.n2 - j0 < 256) ? a.gr.n2 - j0 : 256;
+    const int k = threadIdx.x >> 8, jj = threadIdx.x & 255;
+    if (k < 4 && jj < m) buf[k][jj] = a.fixbuf[(long long)k * a.gr.plane + j0 + jj];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double s = acc[threadIdx.x];
+      for (int q = 0; q < m; q++) s += buf[threadIdx.x][q];
+      acc[threadIdx.x] = s;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    DevScalars* sc = a.sc;
+    for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
+    sc->hz[4] += acc[0] * sc->dt;
+    sc->hz[5] += acc[1] * sc->dt;
+    sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
+  }
   double m1 = 1.e9, m2 = 1.e9;
   for (int b = threadIdx.x; b < a.nblocks_flux; b += blockDim.x) {
     double v1 = a.blockmin[b], v2 = a.blockmin[a.nblocks_flux + b];
@@ -732,7 +765,7 @@ void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const St
 void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)
 {
   if (mixed) launch_horizon_mixed(s, a, pv);
-  else k_horizon<double><<<1, 1024, 0, s>>>(a, pv);
+  else k_horizon<double><<<(a.gr.n2 + 63) / 64, 64, 0, s>>>(a, pv);
 }
 
 }  // namespace harm

@@ -352,61 +352,42 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
 
 // ---------------------------------------------------------------- horizon
 // diag_flux() for the global region's inner x1 face (diag.c:576-833): the
-// face fluxes in diagnostic form (UtoU UEVOLVE->UDIAG) summed over j, the
-// energy-equation stress terms 3 and 6 from the zone-centred state, and
-// pcum += pdot * dt.  The per-j terms are formed in parallel; the sums run in
-// j order on one thread, as the reference's loop does, so they are exact.
+// face fluxes in diagnostic form (UtoU UEVOLVE->UDIAG) and the energy-
+// equation stress terms 3 and 6 from the zone-centred state, per j, in
+// parallel, into the repair scratch (idle at this point of the step):
+// fixbuf[k * plane + j], k = 0..3.  k_dt_finalize then sums them in j order,
+// as the reference's loop does (so the sums are exact), and adds pcum +=
+// pdot * dt.
 template <typename FT>
-__global__ void __launch_bounds__(1024) k_horizon(StepArgs a, const double* __restrict__ pv)
+__global__ void __launch_bounds__(64) k_horizon(StepArgs a, const double* __restrict__ pv)
 {
   const FT* F1 = reinterpret_cast<const FT*>(a.F1);
-  __shared__ double t[4][1024];
-  __shared__ double acc[4];
-  const int n2 = a.gr.n2;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.gr.n2) return;
   const long long pl = a.gr.plane;
   const double surface = a.pp.dx2 * (2.0 * 3.14159265358979323846);
-  if (threadIdx.x < 4) acc[threadIdx.x] = 0.;
-  for (int j0 = 0; j0 < n2; j0 += 1024) {
-    const int j = j0 + threadIdx.x;
-    if (j < n2) {
-      const long long z = a.gr.at(0, j);
-      const double gf = gdet_at(a, FACE1, z);
-      const double Fr = (double)F1[RHO * pl + z] * surface, Fu = (double)F1[UU * pl + z] * surface;
-      const double gr = Fr / gf;
-      double gu = Fu / gf;
-      gu += -gr;
-      t[0][threadIdx.x] = gr * gf;
-      t[1][threadIdx.x] = gu * gf;
-      double pr[NPR];
+  const long long z = a.gr.at(0, j);
+  const double gf = gdet_at(a, FACE1, z);
+  const double Fr = (double)F1[RHO * pl + z] * surface, Fu = (double)F1[UU * pl + z] * surface;
+  const double gr = Fr / gf;
+  double gu = Fu / gf;
+  gu += -gr;
+  double* t = a.fixbuf;
+  t[j] = gr * gf;
+  t[pl + j] = gu * gf;
+  double pr[NPR];
 #pragma unroll
-      for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
-      Geo<double> g;
-      load_geo(a, CENT, z, g);
-      State<double> q;
-      state_of(pr, g, q);
-      double bsq = 0;
+  for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  State<double> q;
+  state_of(pr, g, q);
+  double bsq = 0;
 #pragma unroll
-      for (int l = 0; l < 4; l++) bsq += (q.bcon[l]) * (q.bcov[l]);
-      const double surgdet = (g.g) * surface;
-      t[2][threadIdx.x] = bsq * (q.ucon[1]) * (q.ucov[0]) * surgdet;
-      t[3][threadIdx.x] = -(q.bcon[1]) * (q.bcov[0]) * surgdet;
-    }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double s = acc[threadIdx.x];
-      const int m = (n2 - j0 < 1024) ? n2 - j0 : 1024;
-      for (int k = 0; k < m; k++) s += t[threadIdx.x][k];
-      acc[threadIdx.x] = s;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    DevScalars* sc = a.sc;
-    for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
-    sc->hz[4] += acc[0] * sc->dt;
-    sc->hz[5] += acc[1] * sc->dt;
-    sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
-  }
+  for (int l = 0; l < 4; l++) bsq += (q.bcon[l]) * (q.bcov[l]);
+  const double surgdet = (g.g) * surface;
+  t[2 * pl + j] = bsq * (q.ucon[1]) * (q.ucov[0]) * surgdet;
+  t[3 * pl + j] = -(q.bcon[1]) * (q.bcov[0]) * surgdet;
 }
 
 }  // namespace harm

@@ -26,6 +26,9 @@ void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArg
   else k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
 }
 
-void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv) { k_horizon<float><<<1, 1024, 0, s>>>(a, pv); }
+void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv)
+{
+  k_horizon<float><<<(a.gr.n2 + 63) / 64, 64, 0, s>>>(a, pv);
+}
 
 }  // namespace harm
