@@ -23,6 +23,7 @@
 
 namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
+__global__ void k_bsqflags_ring(StepArgs a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
 __global__ void k_gammacheck(StepArgs a, double* pv, int poledeath);
@@ -120,6 +121,7 @@ struct harm_ctx {
     a.pp.currents = cfg.currents;
     a.rec_pinv = nullptr;
     a.rec_fixset = nullptr;
+    a.bsqf_fused = nullptr;
     a.nblocks_flux = nblocks_flux;
     a.sc = d_sc;
     return a;
@@ -189,13 +191,22 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
   cudaStream_t s = c->stream;
   const size_t pbytes = (size_t)NPR * c->gr.plane * sizeof(double), fbytes = (size_t)c->gr.plane * sizeof(int);
   if (rec) cudaMemcpyAsync(rec->pn, c->d_p, pbytes, cudaMemcpyDeviceToDevice, s);
-  k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
+  // b^2 flags of the step's p: FP64 GRMHD sets the active zones' inside the
+  // first substep's k_update (from the state it forms anyway), the ring here
+  const bool fuse_bsq = (c->cfg.precision == HARM_PREC_FP64) && (c->cfg.eom == HARM_EOM_GRMHD);
+  if (fuse_bsq) {
+    const int nring = 2 * (n1 + 2) + 2 * n2;
+    k_bsqflags_ring<<<(nring + 127) / 128, 128, 0, s>>>(a, c->d_p);
+  } else {
+    k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
+  }
   T.mark(s, KC_BSQ);
   for (int sub = 0; sub < 2; sub++) {
     if (rec) {
       a.rec_pinv = rec->pinv[sub];
       a.rec_fixset = rec->fixset[sub];
     }
+    a.bsqf_fused = (fuse_bsq && sub == 0) ? a0.bsqf : nullptr;
     const double* pi = c->d_p;
     const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;

@@ -79,11 +79,27 @@ struct StepArgs {
   int* worklist;         // deferred zone indices (capacity: one plane)
   const double* pstep;   // the step's p (the star's inner ghost field is held at it)
   double* cur;           // currents (25 planes): F^{i t} ring 3x3, F^{i r} 3, F^{i h} 3, fcon 6, jcon 4
+  unsigned char* bsqf_fused;  // (or null) k_update sets the b^2 flags of its zones here (first substep, FP64)
   double* rec_pinv;      // adjoint recording (or null): inverted prims before the floors, 8 planes
   unsigned char* rec_fixset;  // adjoint recording (or null): neighbour set of each repaired zone
   int nblocks_flux;
   DevScalars* sc;
 };
+
+// get_bsqflags (fixup.c:1214-1233): (b^2/rho flag) | (b^2/u flag) << 2 of a
+// zone-centred state
+__device__ __forceinline__ unsigned char bsq_flag(const StepArgs& a, const double* pr, const State<double>& q)
+{
+  const double bsq = dot4(q.bcon, q.bcov);
+  int f0, f3;
+  if (bsq / pr[RHO] > a.pp.bsqorholimit) f0 = 2;
+  else if (bsq / pr[RHO] > 0.9 * a.pp.bsqorholimit) f0 = 1;
+  else f0 = 0;
+  if (bsq / pr[UU] > a.pp.bsqoulimit) f3 = 2;
+  else if (bsq / pr[UU] > 0.9 * a.pp.bsqoulimit) f3 = 1;
+  else f3 = 0;
+  return (unsigned char)(f0 | (f3 << 2));
+}
 
 __device__ __forceinline__ void report_fail(DevScalars* sc, int code, int i, int j)
 {

@@ -36,15 +36,40 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
   load_geo(a, CENT, z, g);
   State<double> q;
   state_of(pr, g, q);
-  double bsq = dot4(q.bcon, q.bcov);
-  int f0, f3;
-  if (bsq / pr[RHO] > a.pp.bsqorholimit) f0 = 2;
-  else if (bsq / pr[RHO] > 0.9 * a.pp.bsqorholimit) f0 = 1;
-  else f0 = 0;
-  if (bsq / pr[UU] > a.pp.bsqoulimit) f3 = 2;
-  else if (bsq / pr[UU] > 0.9 * a.pp.bsqoulimit) f3 = 1;
-  else f3 = 0;
-  a.bsqf[z] = (unsigned char)(f0 | (f3 << 2));
+  a.bsqf[z] = bsq_flag(a, pr, q);
+}
+
+// the same for the ring of zones one outside the active grid only (i or j
+// in {-1, N}); the first substep's k_update sets the active zones' flags
+__global__ void k_bsqflags_ring(StepArgs a, const double* __restrict__ pv)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  int i, j;
+  if (t < n1 + 2) {
+    i = t - 1;
+    j = -1;
+  } else if (t < 2 * (n1 + 2)) {
+    i = t - (n1 + 2) - 1;
+    j = n2;
+  } else if (t < 2 * (n1 + 2) + n2) {
+    i = -1;
+    j = t - 2 * (n1 + 2);
+  } else if (t < 2 * (n1 + 2) + 2 * n2) {
+    i = n1;
+    j = t - 2 * (n1 + 2) - n2;
+  } else {
+    return;
+  }
+  const long long z = a.gr.at(i, j);
+  double pr[NPR];
+#pragma unroll
+  for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * a.gr.plane + z);
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  State<double> q;
+  state_of(pr, g, q);
+  a.bsqf[z] = bsq_flag(a, pr, q);
 }
 
 // The deferred inversions of k_update, redone with the full iteration limit.

@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
     State<double> q;
     state_of(pr, g, q);
     flux_of<double, FFDE>(pr, q, 0, g, gam, U);
+    if (a.bsqf_fused) a.bsqf_fused[z] = bsq_flag(a, pr, q);  // get_bsqflags of the step's p
   }
   double dUg[NPR];
   {
