@@ -1268,7 +1268,7 @@ int harm_get_fluxes(harm_ctx* c, double* F1, double* F2)
 // this file-scope device array, so the call allocates nothing.  Every device
 // that loads the library holds one copy of it until the process exits.
 static constexpr long long NOALLOC_MAX_PLANE = 5632;  // pitch * (n2 + 6): 64 x 64 interior zones fit
-static constexpr int NOALLOC_MAX_BLOCKS = 256;        // x1/x2 flux blocks of 32 x 4 zones
+static constexpr int NOALLOC_MAX_BLOCKS = 256;        // x1/x2 flux blocks (k_flux grid)
 static constexpr long long NA_DPLANES = 39;  // pk0 8, F1 8, F2 8, emf, gammacheck, fixbuf 5, ubuf 8
 static constexpr long long NA_OFF_BLOCKMIN = NA_DPLANES * NOALLOC_MAX_PLANE;
 static constexpr long long NA_OFF_SCALARS = NA_OFF_BLOCKMIN + 2 * NOALLOC_MAX_BLOCKS;

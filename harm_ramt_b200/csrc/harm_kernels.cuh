@@ -136,7 +136,7 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 // k_flux blocks: 32 zones along x1 (one warp) x FLUX_BY rows.  Neighbouring
 // blocks overlap by one zone along x1, so that each covers FLUX_BX x1 faces
 // without recomputing a neighbour's interface state.
-constexpr int FLUX_BY = 4, FLUX_BX = 31;
+constexpr int FLUX_BY = 16, FLUX_BX = 31;
 inline dim3 flux_grid(int n1, int n2) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + FLUX_BY - 1) / FLUX_BY); }
 
 // plane offsets of the currents block

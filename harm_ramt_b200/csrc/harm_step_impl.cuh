@@ -119,10 +119,11 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // FLUX_BX = 31 along x1): lane 0 only lends its right state, and its faces
 // are the previous block's (block 0's lane 0 is zone -1, which has no x1
 // face but an x2 face).
-// FP64: at most 128 registers (4 blocks per SM); the register-light FP32
-// faces of the mixed form are left unconstrained
+// 16 rows per block, so that only one row in 16 recomputes its x2
+// neighbour.  512 threads per block: at most 128 registers a thread (one
+// block per SM), for the FP64 and the FP32 (mixed) faces alike.
 template <typename T, bool PARA, bool FFDE>
-__global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 4 : 1) k_flux(StepArgs a, const double* __restrict__ pb)
+__global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 512 / (32 * FLUX_BY) : 1) k_flux(StepArgs a, const double* __restrict__ pb)
 {
   __shared__ double sh[2][32];
   __shared__ T shr[NPR][FLUX_BY][32];
