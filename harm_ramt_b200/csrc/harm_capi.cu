@@ -77,6 +77,7 @@ struct harm_ctx {
   unsigned char *d_bsqf, *d_chk;
   DevScalars* d_sc;
   int nblocks_flux;
+  int flux_by;       // k_flux rows per block (flux_rows)
   bool geo_ok;
   cudaGraph_t graph;
   cudaGraphExec_t gexec;
@@ -185,7 +186,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
   const StepArgs a0 = c->args();
   StepArgs a = a0;
   const int n1 = c->cfg.n1, n2 = c->cfg.n2;
-  const dim3 fb(32, FLUX_BY);     // k_flux's shape is fixed by its warp/shared-memory state sharing
+  const dim3 fb(32, c->flux_by);  // k_flux's shape is fixed by its warp/shared-memory state sharing
   const dim3 b = c->tile_small;   // the other stencil kernels
   const dim3 ub = c->tile_update;
   cudaStream_t s = c->stream;
@@ -214,7 +215,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     const int mixed = c->cfg.precision == HARM_PREC_MIXED;
     const int ffde = c->cfg.eom == HARM_EOM_FFDE;
     const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2), fb, s, a, pb);
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2, c->flux_by), fb, s, a, pb);
     T.mark(s, KC_FLUX);
     launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
@@ -323,7 +324,8 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   c->gr.plane = (long long)c->gr.pitch * c->gr.rows;
   const size_t pd = (size_t)c->gr.plane * sizeof(double);
   const dim3 b(32, 4);
-  dim3 gf = flux_grid(cfg->n1, cfg->n2);
+  c->flux_by = flux_rows(cfg->n1, cfg->n2);
+  dim3 gf = flux_grid(cfg->n1, cfg->n2, c->flux_by);
   c->nblocks_flux = gf.x * gf.y;
   c->tile_update = dim3(32, 4);
   c->tile_small = dim3(32, 4);
@@ -1301,7 +1303,8 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.gr.rows = c.n2m;
   c.gr.plane = (long long)c.gr.pitch * c.gr.rows;
   const dim3 b(32, 4);
-  const dim3 gf = flux_grid(cfg->n1, cfg->n2);
+  c.flux_by = flux_rows(cfg->n1, cfg->n2);
+  const dim3 gf = flux_grid(cfg->n1, cfg->n2, c.flux_by);
   c.nblocks_flux = gf.x * gf.y;
   c.tile_update = dim3(32, 4);
   c.tile_small = dim3(32, 4);

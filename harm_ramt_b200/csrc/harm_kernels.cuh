@@ -133,11 +133,19 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
 
-// k_flux blocks: 32 zones along x1 (one warp) x FLUX_BY rows.  Neighbouring
+// k_flux blocks: 32 zones along x1 (one warp) x 4 or 16 rows.  Neighbouring
 // blocks overlap by one zone along x1, so that each covers FLUX_BX x1 faces
-// without recomputing a neighbour's interface state.
-constexpr int FLUX_BY = 16, FLUX_BX = 31;
-inline dim3 flux_grid(int n1, int n2) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + FLUX_BY - 1) / FLUX_BY); }
+// without recomputing a neighbour's interface state.  16 rows leave less
+// x2 recomputation (one row in 16) but hold one 512-thread block per SM:
+// they are used when that grid still fills three waves of the 148 SMs,
+// 4 rows (four 128-thread blocks per SM) on smaller grids.
+constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = 16;
+inline dim3 flux_grid(int n1, int n2, int by) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + by - 1) / by); }
+inline int flux_rows(int n1, int n2)
+{
+  const dim3 g = flux_grid(n1, n2, FLUX_BY_LARGE);
+  return (g.x * g.y >= 3 * 148) ? FLUX_BY_LARGE : FLUX_BY_SMALL;
+}
 
 // plane offsets of the currents block
 constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 21, CUR_NPLANES = 25;

@@ -766,10 +766,10 @@ void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, 
 {
   if (mixed) launch_flux_mixed(para, ffde, g, b, s, a, pb);
   else if (ffde) {
-    if (para) k_flux<double, true, true><<<g, b, 0, s>>>(a, pb);
-    else k_flux<double, false, true><<<g, b, 0, s>>>(a, pb);
-  } else if (para) k_flux<double, true, false><<<g, b, 0, s>>>(a, pb);
-  else k_flux<double, false, false><<<g, b, 0, s>>>(a, pb);
+    if (para) flux_rows_launch<double, true, true>(g, b, s, a, pb);
+    else flux_rows_launch<double, false, true>(g, b, s, a, pb);
+  } else if (para) flux_rows_launch<double, true, false>(g, b, s, a, pb);
+  else flux_rows_launch<double, false, false>(g, b, s, a, pb);
 }
 
 void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a)

@@ -119,17 +119,16 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // FLUX_BX = 31 along x1): lane 0 only lends its right state, and its faces
 // are the previous block's (block 0's lane 0 is zone -1, which has no x1
 // face but an x2 face).
-// 16 rows per block, so that only one row in 16 recomputes its x2
-// neighbour.  512 threads per block: at most 128 registers a thread (one
-// block per SM), for the FP64 and the FP32 (mixed) faces alike.
-template <typename T, bool PARA, bool FFDE>
-__global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 512 / (32 * FLUX_BY) : 1) k_flux(StepArgs a, const double* __restrict__ pb)
+// BY = 4 or 16 rows per block (flux_rows).  FP64 faces: at most 128
+// registers a thread either way (512 threads per SM).
+template <typename T, bool PARA, bool FFDE, int BY>
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 1) k_flux(StepArgs a, const double* __restrict__ pb)
 {
   __shared__ double sh[2][32];
-  __shared__ T shr[NPR][FLUX_BY][32];
+  __shared__ T shr[NPR][BY][32];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = blockIdx.x * FLUX_BX + tx - 1;
-  const int j = blockIdx.y * FLUX_BY + ty - 1;
+  const int j = blockIdx.y * BY + ty - 1;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   const bool in = (i <= n1) && (j <= n2);
   const bool own = (tx > 0) || (blockIdx.x == 0);  // lane 0 of a later block repeats a zone
@@ -186,6 +185,14 @@ __global__ void __launch_bounds__(32 * FLUX_BY, (sizeof(T) == 8) ? 512 / (32 * F
     a.blockmin[b] = dt1;
     a.blockmin[a.nblocks_flux + b] = dt2;
   }
+}
+
+// the k_flux instance of the block's row count (b.y)
+template <typename T, bool PARA, bool FFDE>
+inline void flux_rows_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+{
+  if (b.y == FLUX_BY_LARGE) k_flux<T, PARA, FFDE, FLUX_BY_LARGE><<<g, b, 0, s>>>(a, pb);
+  else k_flux<T, PARA, FFDE, FLUX_BY_SMALL><<<g, b, 0, s>>>(a, pb);
 }
 
 // flux_ct corner EMF, step_ch.c:1214-1234, over i in [0,N1], j in [0,N2].

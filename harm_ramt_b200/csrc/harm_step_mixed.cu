@@ -11,10 +11,10 @@ namespace harm {
 void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
 {
   if (ffde) {
-    if (para) k_flux<float, true, true><<<g, b, 0, s>>>(a, pb);
-    else k_flux<float, false, true><<<g, b, 0, s>>>(a, pb);
-  } else if (para) k_flux<float, true, false><<<g, b, 0, s>>>(a, pb);
-  else k_flux<float, false, false><<<g, b, 0, s>>>(a, pb);
+    if (para) flux_rows_launch<float, true, true>(g, b, s, a, pb);
+    else flux_rows_launch<float, false, true>(g, b, s, a, pb);
+  } else if (para) flux_rows_launch<float, true, false>(g, b, s, a, pb);
+  else flux_rows_launch<float, false, false>(g, b, s, a, pb);
 }
 
 void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a) { k_emf<float><<<g, b, 0, s>>>(a); }
