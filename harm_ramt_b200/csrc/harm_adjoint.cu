@@ -340,8 +340,9 @@ __global__ void k_adj_corner(StepArgs a, const double* __restrict__ lam_dU, doub
 // planes each, indexed by the face) get the adjoints of its left and right
 // interface states, zero where the face carries none.  k_adj_recon takes
 // them through the reconstructions.
+template <int dir>
 __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const double* __restrict__ lam_dU,
-                            const double* __restrict__ lam_e, double* sl, double* sr, int dir, double seed_fac)
+                            const double* __restrict__ lam_e, double* sl, double* sr, double seed_fac)
 {
   const double seed_mdot = seed_fac * a.sc->dt;
   const int i = blockIdx.x * blockDim.x + threadIdx.x - (dir == 2 ? 1 : 0);
@@ -450,8 +451,9 @@ __global__ void k_adj_faces(StepArgs a, const double* __restrict__ pb, const dou
 // without bound; any resolvable perturbation sees the tie's rows.
 constexpr double B_NOISE = 1e-10;
 
+template <int dir>
 __global__ void k_adj_recon(StepArgs a, const double* __restrict__ pb, const double* __restrict__ sl,
-                            const double* __restrict__ sr, double* lam_b, int dir)
+                            const double* __restrict__ sr, double* lam_b)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
@@ -527,5 +529,14 @@ __global__ void k_dot_active(StepArgs a, const double* __restrict__ lam, const d
     out[blockIdx.y * gridDim.x + blockIdx.x] = b;
   }
 }
+
+// the direction is a template parameter: every dir-indexed state component
+// is then a constant index and stays in registers
+template __global__ void k_adj_faces<1>(StepArgs, const double*, const double*, const double*, double*, double*,
+                                        double);
+template __global__ void k_adj_faces<2>(StepArgs, const double*, const double*, const double*, double*, double*,
+                                        double);
+template __global__ void k_adj_recon<1>(StepArgs, const double*, const double*, const double*, double*);
+template __global__ void k_adj_recon<2>(StepArgs, const double*, const double*, const double*, double*);
 
 }  // namespace harm

@@ -571,10 +571,14 @@ HD_INLINE void adj_source(const double* p, const Geo<double>& g, double gam, con
   state_of(p, g, q);
   StateAdj qb;
   qb.zero();
+  // unrolled: jj indexes the state components as a constant
+#pragma unroll
   for (int jj = 0; jj < 4; jj++) {
     double rowb[4];
+#pragma unroll
     for (int k = 0; k < 4; k++) {
       double s = 0.;
+#pragma unroll
       for (int l = 0; l < 4; l++) s += dUgb[l] * g.g * conn40[k * 10 + sym(l, jj)];
       rowb[k] = s;
     }
@@ -591,6 +595,7 @@ HD_INLINE void primtoU_jacobian5(const double* p, const Geo<double>& g, double g
 {
   State<double> q;
   state_of(p, g, q);
+#pragma unroll
   for (int r = 0; r < 5; r++) {
     double Fb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
     Fb[r] = 1.;
@@ -608,40 +613,89 @@ HD_INLINE void primtoU_jacobian5(const double* p, const Geo<double>& g, double g
 // depend on rho..u3, so the rho..u3 columns give a 5 x 5 system in x_0..4
 // (Gaussian elimination with partial pivoting) and the B columns then give
 // x_B = (b_B - sum_r J[r][B] x_r) / g.  Returns nonzero for a singular
-// matrix.
+// matrix.  The matrices stay in registers: every index is a compile-time
+// constant after unrolling, the pivot row swapped in by selects.
 HD_INLINE int ift_solve(const double* p, const Geo<double>& g, double gam, const double* b, double* x)
 {
-  double J[5][NPR];
-  primtoU_jacobian5(p, g, gam, J);
-  double A[5][6];
-  for (int r = 0; r < 5; r++) {
-    for (int c = 0; c < 5; c++) A[r][c] = J[c][r];
-    A[r][5] = b[r];
-  }
-  for (int col = 0; col < 5; col++) {
-    int piv = col;
-    for (int r = col + 1; r < 5; r++)
-      if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
-    if (A[piv][col] == 0.0) return 1;
-    if (piv != col)
-      for (int c = 0; c < 6; c++) {
-        const double t = A[col][c];
-        A[col][c] = A[piv][c];
-        A[piv][c] = t;
+  // A = the transposed rho..u3 block with b beside it; JB[r] = dU_r/dB
+  double A[5][6], JB[5][3];
+  {
+    State<double> q;
+    state_of(p, g, q);
+    // one reverse sweep per row (a loop the compiler keeps rolled: the rows
+    // shift in from the end, so that A and JB are indexed by constants)
+    for (int r = 0; r < 5; r++) {
+      double Fb[NPR];
+#pragma unroll
+      for (int k = 0; k < NPR; k++) Fb[k] = (k == r) ? 1. : 0.;
+      StateAdj qb;
+      qb.zero();
+      double row[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+      adj_flux(p, q, 0, g, gam, Fb, qb, row);
+      adj_state(p, g, q, qb, row);
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+#pragma unroll
+        for (int c = 0; c < 5; c++) A[c][m] = A[c][m + 1];
+#pragma unroll
+        for (int c = 0; c < 3; c++) JB[m][c] = JB[m + 1][c];
       }
-    for (int r = col + 1; r < 5; r++) {
-      const double f = A[r][col] / A[col][col];
-      for (int c = col; c < 6; c++) A[r][c] -= f * A[col][c];
+#pragma unroll
+      for (int c = 0; c < 5; c++) A[c][4] = row[c];
+#pragma unroll
+      for (int c = 0; c < 3; c++) JB[4][c] = row[B1 + c];
     }
   }
-  for (int r = 4; r >= 0; r--) {
+#pragma unroll
+  for (int r = 0; r < 5; r++) A[r][5] = b[r];
+  // fixed trip counts with the triangular ranges as conditions: nvcc then
+  // unrolls every loop and keeps A in registers
+#pragma unroll
+  for (int col = 0; col < 5; col++) {
+    int piv = col;
+    double big = fabs(A[col][col]);
+#pragma unroll
+    for (int r = 1; r < 5; r++)
+      if (r > col && fabs(A[r][col]) > big) {
+        piv = r;
+        big = fabs(A[r][col]);
+      }
+    if (big == 0.0) return 1;
+#pragma unroll
+    for (int r = 1; r < 5; r++) {
+      if (r <= col) continue;
+      const bool sw = (r == piv);
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        if (c < col) continue;
+        const double t = A[col][c], u = A[r][c];
+        A[col][c] = sw ? u : t;
+        A[r][c] = sw ? t : u;
+      }
+    }
+#pragma unroll
+    for (int r = 1; r < 5; r++) {
+      if (r <= col) continue;
+      const double f = A[r][col] / A[col][col];
+#pragma unroll
+      for (int c = 0; c < 6; c++)
+        if (c >= col) A[r][c] -= f * A[col][c];
+    }
+  }
+#pragma unroll
+  for (int rr = 0; rr < 5; rr++) {
+    const int r = 4 - rr;
     double s = A[r][5];
-    for (int c = r + 1; c < 5; c++) s -= A[r][c] * x[c];
+#pragma unroll
+    for (int c = 1; c < 5; c++)
+      if (c > r) s -= A[r][c] * x[c];
     x[r] = s / A[r][r];
   }
+#pragma unroll
   for (int c = B1; c <= B3; c++) {
     double s = b[c];
-    for (int r = 0; r < 5; r++) s -= J[r][c] * x[r];
+#pragma unroll
+    for (int r = 0; r < 5; r++) s -= JB[r][c - B1] * x[r];
     x[c] = s / g.g;
   }
   return 0;

@@ -46,9 +46,11 @@ __global__ void k_adj_update(StepArgs a, const double* lam, const double* pinv, 
 __global__ void k_adj_upi(StepArgs a, const double* ubar, const double* pi, double* lam_pi);
 __global__ void k_adj_source(StepArgs a, const double* pb, const double* lam_dU, double* lam_b);
 __global__ void k_adj_corner(StepArgs a, const double* lam_dU, double* lam_e);
+template <int dir>
 __global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, const double* lam_e, double* sl,
-                            double* sr, int dir, double seed_fac);
-__global__ void k_adj_recon(StepArgs a, const double* pb, const double* sl, const double* sr, double* lam_b, int dir);
+                            double* sr, double seed_fac);
+template <int dir>
+__global__ void k_adj_recon(StepArgs a, const double* pb, const double* sl, const double* sr, double* lam_b);
 __global__ void k_set_dt(StepArgs a, const double* dts, int k);
 __global__ void k_get_dt(StepArgs a, double* dts, int k);
 __global__ void k_axpy(double* y, const double* x, long long n);
@@ -937,10 +939,10 @@ void adjoint_substep(harm_ctx* c, AdjWork& w, const Rec& r, int sub, double* lam
   k_adj_source<<<grid2(n1, n2, b), b, 0, s>>>(a, pb, w.LdU, out);
   k_adj_corner<<<grid2(n1 + 1, n2 + 1, b), b, 0, s>>>(a, w.LdU, w.Le);
   // the face-state adjoints go to Lsnap (free after the update) and Sr
-  k_adj_faces<<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, 1, seed_fac);
-  k_adj_recon<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out, 1);
-  k_adj_faces<<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, 2, 0.);
-  k_adj_recon<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out, 2);
+  k_adj_faces<1><<<grid2(n1 + 1, n2 + 2, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, seed_fac);
+  k_adj_recon<1><<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out);
+  k_adj_faces<2><<<grid2(n1 + 2, n2 + 1, b), b, 0, s>>>(a, pb, w.LdU, w.Le, w.Lsnap, w.Sr, 0.);
+  k_adj_recon<2><<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pb, w.Lsnap, w.Sr, out);
 }
 
 // step n's adjoint from its record r and its output state pout (p^{n+1}),
