@@ -34,6 +34,10 @@ FLUX_LAXF, FLUX_HLL = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 EOM_GRMHD, EOM_FFDE = 0, 1
 BC_TORUS, BC_STAR = 0, 1
+# con-to-prim methods of Utoprimgen_pick (step_ch.h:39-53); INV_CHAIN: the
+# whole Utoprimgen with the UTOPRIMTRYAGAIN retry chain
+INV_5D1, INV_2D, INV_1D, INV_1DOPT, INV_1DFINAL, INV_2DFINAL, INV_5D2, INV_CHAIN = 0, 2, 3, 4, 5, 6, 7, -1
+TRYAGAIN_CHAIN = (INV_5D1, INV_2D, INV_1D, INV_1DOPT, INV_1DFINAL, INV_2DFINAL, INV_5D2)
 
 _ERRORS = {0: "ok", 1: "invalid argument", 2: "no usable CUDA device (sm_100 required)", 3: "CUDA runtime error",
            4: "device allocation failed", 5: "geometry tables missing or not symmetric",
@@ -57,7 +61,7 @@ class _Config(ctypes.Structure):
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
                 ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
                 ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
-                ("omegastar", ctypes.c_double), ("currents", ctypes.c_int)]
+                ("omegastar", ctypes.c_double), ("currents", ctypes.c_int), ("tryagain", ctypes.c_int)]
 
 
 class _DumpHeader(ctypes.Structure):
@@ -94,7 +98,7 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
            "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
            "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt",
-           "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint"]
+           "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint", "harm_invert_zones"]
 
 
 def load_library(path=None):
@@ -122,6 +126,7 @@ def load_library(path=None):
     lib.harm_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]
     lib.harm_set_end_time.argtypes = [vp, ctypes.c_double]
     lib.harm_step.argtypes = [vp, ctypes.c_int]
+    lib.harm_invert_zones.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, dp, dp, ip]
     lib.harm_sync.argtypes = [vp, ctypes.POINTER(_Status)]
     lib.harm_get_fluxes.argtypes = [vp, dp, dp]
     lib.harm_destroy.argtypes = [vp]
@@ -250,13 +255,14 @@ class HarmGPU:
 
     def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
-                 precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0, currents=False):
+                 precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0, currents=False,
+                 tryagain=False):
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
         self.safe = safe
         cfg = _Config(n1, n2, lim, fluxmethod, eom, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                      bsqorholimit, bsqoulimit, tf, bc, omegastar, int(bool(currents)))
+                      bsqorholimit, bsqoulimit, tf, bc, omegastar, int(bool(currents)), int(bool(tryagain)))
         h = ctypes.c_void_p()
         _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
         self._h = h
@@ -327,6 +333,20 @@ class HarmGPU:
             self.step_ch(min(max(k, 1), max_chunk))
             st = self.sync()
         return st
+
+    def invert_zones(self, which, zones, U, guess):
+        """One con-to-prim method of Utoprimgen_pick (step_ch.c:583-600;
+        which: INV_5D1 ... INV_5D2, or INV_CHAIN for the whole Utoprimgen with
+        the UTOPRIMTRYAGAIN retry chain) on the device at the given active
+        zones (n x 2 array of i, j), U the evolved conserved vectors (n x 8),
+        guess the initial primitives (n x 8).  Returns (primitives, pflag)."""
+        zones = np.ascontiguousarray(zones, dtype=np.int32).reshape(-1, 2)
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(-1, NPR)
+        pr = np.ascontiguousarray(guess, dtype=np.float64).reshape(-1, NPR).copy()
+        fl = np.zeros(len(zones), dtype=np.int32)
+        _check(self.lib.harm_invert_zones(self._h, int(which), len(zones), _ip(zones), _dp(U), _dp(pr), _ip(fl)),
+               "harm_invert_zones")
+        return pr, fl
 
     def step_ch(self, nsteps=1):
         """Enqueue nsteps reference steps (asynchronous)."""

@@ -52,6 +52,7 @@ __global__ void k_adj_faces(StepArgs a, const double* pb, const double* lam_dU, 
 template <int dir>
 __global__ void k_adj_recon(StepArgs a, const double* pb, const double* sl, const double* sr, double* lam_b);
 __global__ void k_set_dt(StepArgs a, const double* dts, int k);
+__global__ void k_invert_zones(StepArgs a, int which, int nz, const int* zones, const double* U, double* pr, int* pfl);
 __global__ void k_get_dt(StepArgs a, double* dts, int k);
 __global__ void k_axpy(double* y, const double* x, long long n);
 __global__ void k_mask_ghosts(StepArgs a, double* lam);
@@ -122,6 +123,7 @@ struct harm_ctx {
     a.pstep = d_p;
     a.cur = d_cur;
     a.pp.currents = cfg.currents;
+    a.pp.tryagain = cfg.tryagain;
     a.rec_pinv = nullptr;
     a.rec_fixset = nullptr;
     a.bsqf_fused = nullptr;
@@ -307,6 +309,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
   if (cfg->eom != HARM_EOM_GRMHD && cfg->eom != HARM_EOM_FFDE) return HARM_EINVAL;
   if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
+  if ((cfg->tryagain != 0 && cfg->tryagain != 1) || (cfg->tryagain && cfg->eom != HARM_EOM_GRMHD)) return HARM_EINVAL;
   int dev = 0, ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HARM_ENODEVICE;
   CK(cudaGetDevice(&dev));
@@ -495,6 +498,39 @@ int harm_bound_prims(harm_ctx* c)
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return HARM_OK;
+}
+
+int harm_invert_zones(harm_ctx* c, int which, int nz, const int* zones, const double* U, double* pr, int* pflag)
+{
+  if (!c || nz < 0 || (nz > 0 && (!zones || !U || !pr || !pflag))) return HARM_EINVAL;
+  if (c->cfg.eom != HARM_EOM_GRMHD || which < -1 || which == 1 || which > 7) return HARM_EINVAL;
+  for (int k = 0; k < nz; k++)
+    if (zones[2 * k] < 0 || zones[2 * k] >= c->cfg.n1 || zones[2 * k + 1] < 0 || zones[2 * k + 1] >= c->cfg.n2)
+      return HARM_EINVAL;
+  if (nz == 0) return HARM_OK;
+  int* dz = nullptr;
+  double *dU = nullptr, *dp = nullptr;
+  int* df = nullptr;
+  int rc = HARM_OK;
+  const size_t nd = (size_t)NPR * nz * sizeof(double);
+  if (cudaMalloc(&dz, 2 * nz * sizeof(int)) != cudaSuccess || cudaMalloc(&dU, nd) != cudaSuccess ||
+      cudaMalloc(&dp, nd) != cudaSuccess || cudaMalloc(&df, nz * sizeof(int)) != cudaSuccess)
+    rc = HARM_ENOMEM;
+  cudaStream_t s = c->stream;
+  if (rc == HARM_OK) {
+    cudaMemcpyAsync(dz, zones, 2 * nz * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dU, U, nd, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dp, pr, nd, cudaMemcpyHostToDevice, s);
+    k_invert_zones<<<(nz + 63) / 64, 64, 0, s>>>(c->args(), which, nz, dz, dU, dp, df);
+    cudaMemcpyAsync(pr, dp, nd, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(pflag, df, nz * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = HARM_ECUDA;
+  }
+  cudaFree(dz);
+  cudaFree(dU);
+  cudaFree(dp);
+  cudaFree(df);
+  return rc;
 }
 
 int harm_set_time(harm_ctx* c, double t, double dt, long long realnstep)
@@ -1038,7 +1074,9 @@ void bound_input(harm_ctx* c)
 
 bool adjoint_supported(const harm_ctx* c)
 {
-  return c->cfg.precision == HARM_PREC_FP64 && c->cfg.eom == HARM_EOM_GRMHD && c->cfg.bc == HARM_BC_TORUS;
+  // the con-to-prim adjoint differentiates the 2D inversion's solution
+  return c->cfg.precision == HARM_PREC_FP64 && c->cfg.eom == HARM_EOM_GRMHD && c->cfg.bc == HARM_BC_TORUS &&
+         !c->cfg.tryagain;
 }
 
 }  // namespace
@@ -1293,6 +1331,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   if (cfg->fluxmethod != HARM_FLUX_HLL && cfg->fluxmethod != HARM_FLUX_LAXF) return HARM_EINVAL;
   if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
   if (cfg->currents) return HARM_EINVAL;  // the diagnostic currents need a context
+  if (cfg->tryagain != 0 && cfg->tryagain != 1) return HARM_EINVAL;
   harm_ctx c;
   memset(&c, 0, sizeof(c));
   c.cfg = *cfg;

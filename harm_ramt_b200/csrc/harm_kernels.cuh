@@ -37,6 +37,7 @@ struct Params {
   int eom;          // 0 GRMHD, 1 FFDE
   int currents;     // 1: Faraday slots and J^mu every step
   int bc;           // 0 torus (bounds.fishmon.c), 1 rotating star (bounds.ns.c)
+  int tryagain;     // 1: the UTOPRIMTRYAGAIN retry chain after a failed 2D inversion
   double cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit, tf;
   double omegastar; // bc 1: angular frequency of the stellar surface
 };

@@ -14,6 +14,7 @@
 //   k_bound/k_poledeath again, and k_dt_finalize after the last substep.
 #include <cuda_runtime.h>
 #include "harm_step_impl.cuh"
+#include "harm_tryagain.cuh"
 
 namespace harm {
 
@@ -74,6 +75,8 @@ __global__ void k_bsqflags_ring(StepArgs a, const double* __restrict__ pv)
 
 // The deferred inversions of k_update, redone with the full iteration limit.
 // A deferred zone's pf slot was not written, so pi still holds its guess.
+// TA: the UTOPRIMTRYAGAIN retry chain follows a failed 2D inversion.
+template <bool TA>
 __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __restrict__ pi, double* __restrict__ pf)
 {
   const int nd = a.sc->ndeferred;
@@ -91,10 +94,47 @@ __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __
     }
     int niter;
     int pfl = utoprim_2d(U, g, pfz, a.pp.gam, a.pp.gammafail, &niter);
+    if (TA && pfl != 0) {
+      double pr0[NPR];
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pr0[k] = pi[k * pl + z];
+      pfl = ta::tryagain_chain(U, g, a.pp.gam, a.pp.gammafail, pr0, pfz, pfl);
+    }
     finish_zone(a, g, z, i, j, pfz, pfl, pf);
     atomicAdd(&a.sc->newton_iters, (unsigned long long)niter);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.sc->ndeferred_total += nd;
+}
+
+// One con-to-prim method (Utoprimgen_pick ids, step_ch.h:39-53), or the
+// whole Utoprimgen with the retry chain (which = -1), at nz listed zones:
+// zones (i, j) pairs, U (evolved form) and pr (guess in, result out) 8 per
+// zone, pfl out.
+__global__ void k_invert_zones(StepArgs a, int which, int nz, const int* __restrict__ zones, const double* __restrict__ U,
+                               double* pr, int* pfl)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nz) return;
+  const long long z = a.gr.at(zones[2 * k], zones[2 * k + 1]);
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  double u[NPR], p[NPR], p0[NPR];
+  for (int m = 0; m < NPR; m++) {
+    u[m] = U[NPR * k + m];
+    p[m] = p0[m] = pr[NPR * k + m];
+  }
+  int code;
+  if (which == ta::M_2D || which < 0) {
+    int niter;
+    code = utoprim_2d(u, g, p, a.pp.gam, a.pp.gammafail, &niter);
+    if (which < 0) code = ta::tryagain_chain(u, g, a.pp.gam, a.pp.gammafail, p0, p, code);
+  } else {
+    double Ug[NPR];
+    ta::evolved_to_geomfree(u, g, Ug);
+    code = ta::pick(which, Ug, g, a.pp.gam, a.pp.gammafail, p);
+  }
+  for (int m = 0; m < NPR; m++) pr[NPR * k + m] = p[m];
+  pfl[k] = code;
 }
 
 // ---------------------------------------------------------------- bounds
@@ -784,7 +824,10 @@ void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const St
   if (mixed) launch_update_mixed(ffde, g, b, s, a, pi, pb, pf, c2);
   else if (ffde) k_update<double, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
   else k_update<double, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
-  if (!ffde) k_update_tail<<<148, 64, 0, s>>>(a, pi, pf);
+  if (!ffde) {
+    if (a.pp.tryagain) k_update_tail<true><<<148, 64, 0, s>>>(a, pi, pf);
+    else k_update_tail<false><<<148, 64, 0, s>>>(a, pi, pf);
+  }
 }
 
 void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)

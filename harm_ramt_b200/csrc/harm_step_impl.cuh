@@ -341,9 +341,10 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
   }
   int niter;
   int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP);
-  if (pfl == NEWTON_DEFERRED) {
+  if (pfl == NEWTON_DEFERRED || (a.pp.tryagain && pfl != 0)) {
     // rare slow inversion: hand the zone to k_update_tail so that this warp
-    // is not held for up to 200 iterations by one lane
+    // is not held for up to 200 iterations by one lane (with the retry
+    // chain on, failed inversions go there too)
 #pragma unroll
     for (int k = 0; k < NPR; k++) a.ubuf[k * pl + z] = U[k];
     a.worklist[atomicAdd(&a.sc->ndeferred, 1)] = (int)z;

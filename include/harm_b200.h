@@ -93,6 +93,11 @@ typedef struct harm_config {
   int currents;         /* 1: the diagnostic currents J^mu and the Faraday
                            tensor F^{mu nu} every step, as step_ch.c:143-156
                            does (WHICHCURRENTCALC 1); 0: not computed */
+  int tryagain;         /* 1: the UTOPRIMTRYAGAIN retry chain (global.h:213,
+                           step_ch.c:608-626): a zone whose 2D inversion fails
+                           is inverted again by 5D1, 2D, 1D, 1D_OPT, 1D_FINAL,
+                           2D_FINAL and 5D2_FINAL in turn until one succeeds;
+                           0: the 2D inversion only (GRMHD only) */
 } harm_config;
 
 typedef struct harm_status {
@@ -135,6 +140,16 @@ int harm_set_time(harm_ctx* ctx, double t, double dt, long long realnstep);
    unclamped next dt, so a run that stopped at the old end time moves on;
    the state and the horizon accumulators are kept. */
 int harm_set_end_time(harm_ctx* ctx, double tf);
+
+/* One con-to-prim method of the reference's Utoprimgen_pick
+   (step_ch.c:583-600): which = 0 5D1, 2 2D, 3 1D, 4 1D_OPT, 5 1D_FINAL,
+   6 2D_FINAL, 7 5D2_FINAL (the ids of step_ch.h:39-53), or -1 for the
+   whole Utoprimgen with the UTOPRIMTRYAGAIN retry chain (step_ch.c:468-640),
+   run on the device at nz active zones: zones holds (i, j) pairs, U the
+   evolved conserved vectors (8 per zone, with sqrt(-g), as the update
+   forms them), pr the guesses in and the results out (8 per zone), pflag
+   the codes out.  Host arrays; synchronous.  GRMHD only. */
+int harm_invert_zones(harm_ctx* ctx, int which, int nz, const int* zones, const double* U, double* pr, int* pflag);
 
 /* Enqueues nsteps full steps of step_ch() on the context's stream
    (asynchronous; the first call captures a CUDA graph of one step). */

@@ -42,6 +42,17 @@ Build patches (each one asserted to apply exactly):
      and turns dump files off.
  13. compiled -O2 -ffp-contract=off -fno-fast-math so that no FMA
      contraction changes the FP64 rounding.
+
+The "torusta" problem is the torus with the UTOPRIMTRYAGAIN chain on
+(step_ch.c:608-626), the build that pins the retry chain.  It differs from
+"torus" in three patches:
+  7'. dudp_calc.c and utoprim_{1d,2d,5d2}_final.c are built: their
+      block-scope static prototypes (and u2p_util.c's, which the last two
+      include) are moved to file scope, where gcc accepts them.
+ 10'. UTOPRIMTRYAGAIN stays 1.
+ 11'. the same cycle-break replacement in the three 1D Newton solvers
+      (utoprim_1d.c:559, utoprim_1d_opt.c:618, utoprim_1d_final.c:580):
+      hr_cycle_break_uniform(x[0], 0.0, n_iter).
 """
 import argparse
 import concurrent.futures as cf
@@ -62,9 +73,15 @@ nrutil.c phys.c ranc.c restart.c set_arrays.c set_grid.c step_ch.c tensor.c utop
 utoprim_2d.c utoprim_1d.c utoprim_1d_opt.c vchar.c transforms.c fail.c utoprim_ldz.c
 init_mpi.c boundmpi.c boundmpiint.c sources.c phys.ffde.c advance.c reconstructeno.c""".split()
 
+# patch 7': the files of the retry chain that gcc rejects as they are
+TRYAGAIN_SRCS = ["dudp_calc.c", "utoprim_1d_final.c", "utoprim_2d_final.c", "utoprim_5d2_final.c"]
+
 PROBLEMS = {
     # Fishbone-Moncrief torus in modified Kerr-Schild coordinates (GRMHD).
     "torus": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c", defs=[]),
+    # the same with the UTOPRIMTRYAGAIN retry chain of inversions on
+    "torusta": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c",
+                    defs=["-DHR_TRYAGAIN"], tryagain=True),
     # Force-free aligned rotator (dipole field, rotating stellar surface) in
     # flat space, spherical polar log-r coordinates (FFDE).
     "dipole": dict(eom="EOMFFDE", mcoord="SPCMINKMETRIC", init="init.ns.c", bounds="bounds.ns.c",
@@ -103,7 +120,8 @@ def patch_tree(bdir, problem, n1, n2):
         t = sub1(t, r"#define N1\s+64", f"#define N1 {n1}", f, regex=True)
         t = sub1(t, r"#define N2\s+64", f"#define N2 {n2}", f, regex=True)
         t = sub1(t, "#define EOMTYPE EOMFFDE", f"#define EOMTYPE {prob['eom']}", f)
-        t = sub1(t, "#define UTOPRIMTRYAGAIN 1", "#define UTOPRIMTRYAGAIN 0", f)
+        if not prob.get("tryagain"):
+            t = sub1(t, "#define UTOPRIMTRYAGAIN 1", "#define UTOPRIMTRYAGAIN 0", f)
         t = sub1(t, "#define MAILWHENDONE 1", "#define MAILWHENDONE 0", f)
         t = sub1(t, "#define PRODUCTION 0", "#define PRODUCTION 1", f)
         return t
@@ -134,6 +152,32 @@ def patch_tree(bdir, problem, n1, n2):
                  '#include "utoprim_2d.h"\nextern FTYPE hr_cycle_break_uniform(FTYPE x0, FTYPE x1, int n_iter);', f)
         return t
     edit("utoprim_2d.c", u2d)
+    if not prob.get("tryagain"):
+        return
+
+    proto = re.compile(r"^[ \t]+(static\s+(?:void|int|FTYPE)\s+\w+\s*\([^;{]*\)\s*;)[ \t]*$", re.M)
+
+    def hoist(anchor):
+        # block-scope static prototypes -> file scope, right after `anchor`
+        def fn(t, f):
+            found = proto.findall(t)
+            if not found:
+                raise SystemExit(f"patch failed in {f}: no block-scope static prototypes")
+            t = proto.sub("", t)
+            decl = "\n".join(dict.fromkeys(found))
+            return sub1(t, anchor, anchor + "\n" + decl + "\n", f)
+        return fn
+    edit("dudp_calc.c", hoist('#include "decs.h"'))
+    edit("u2p_util.c", hoist('//#include "u2p_defs.h"'))
+    edit("utoprim_1d_final.c", hoist("#define NEWT_DIM 1"))
+    edit("utoprim_2d_final.c", hoist("#define NEWT_DIM 2"))
+    edit("utoprim_5d2_final.c", hoist("#define NEWT_DIM 5"))
+
+    def u1d(t, f):
+        t = sub1(t, "randtmp = ( (1.*rand())/(1.*RAND_MAX) );", "randtmp = hr_cycle_break_uniform(x[0], 0.0, n_iter);", f)
+        return "extern double hr_cycle_break_uniform(double x0, double x1, int n_iter);\n" + t
+    for name in ("utoprim_1d.c", "utoprim_1d_opt.c", "utoprim_1d_final.c"):
+        edit(name, u1d)
 
 
 def build(src, problem, n1, n2, jobs, force=False):
@@ -153,7 +197,7 @@ def build(src, problem, n1, n2, jobs, force=False):
             shutil.copyfile(os.path.join(src, name), os.path.join(bdir, name))
     patch_tree(bdir, problem, n1, n2)
     shutil.copyfile(harness, os.path.join(bdir, "hr_harness.c"))
-    srcs = BASE_SRCS + ["hr_harness.c"]
+    srcs = BASE_SRCS + (TRYAGAIN_SRCS if PROBLEMS[problem].get("tryagain") else []) + ["hr_harness.c"]
 
     def cc(name):
         obj = os.path.join(bdir, name[:-2] + ".o")

@@ -88,6 +88,11 @@ struct ho_state {
   double clastdt;     /* and its static lastdt */
   long ncb;
   int fail;
+  /* inputs of the inversions that failed (test fixtures for the retry
+     chain): zone, U in the evolved form, the guess; up to rec_max */
+  int rec_max, rec_n;
+  int *rec_ij;
+  double *rec_U, *rec_pr;
 };
 
 /* ---------------------------------------------------------------- indexing */
@@ -1049,8 +1054,19 @@ static int advance(ho_state *s, const double *pi, const double *pb, double *pf, 
       if (s->c.eom) {
         if ((rc = utoprim_ffde(s, last ? un : Uf, &g, pfz))) return rc;
       } else {
+        double guess[NPR];
+        for (k = 0; k < NPR; k++) guess[k] = pfz[k];
         int pfl = utoprimgen(s, last ? un : Uf, &g, pfz, &s->ncb);
         FL(pflag, i, j)[F_FAIL] = pfl;
+        if (pfl != 0 && s->rec_n < s->rec_max) {
+          s->rec_ij[2 * s->rec_n] = i;
+          s->rec_ij[2 * s->rec_n + 1] = j;
+          for (k = 0; k < NPR; k++) {
+            s->rec_U[NPR * s->rec_n + k] = (last ? un : Uf)[k];
+            s->rec_pr[NPR * s->rec_n + k] = guess[k];
+          }
+          s->rec_n++;
+        }
         /* fixup1zone, fixup.c:274-377 (floors are GRMHD-only, 293) */
         const double *fl = s->floors + zid(s, i, j) * 2;
         if (fl[0] > pfz[RHO]) pfz[RHO] = fl[0];
@@ -1206,6 +1222,7 @@ void ho_destroy(ho_state *s)
   free(s->pk0); free(s->dq); free(s->pl); free(s->pr); free(s->F1); free(s->F2);
   free(s->emf); free(s->prc); free(s->ulast); free(s->unew); free(s->gammacheck);
   free(s->cfar); free(s->fcon); free(s->jcon);
+  free(s->rec_ij); free(s->rec_U); free(s->rec_pr);
   free(s);
 }
 
@@ -1224,6 +1241,32 @@ void ho_get_fluxes(const ho_state *s, double *f1, double *f2)
 }
 
 long ho_ncyclebreak(const ho_state *s) { return s->ncb; }
+
+/* records the inputs of up to max failed inversions from now on */
+int ho_record_failures(ho_state *s, int max)
+{
+  free(s->rec_ij);
+  free(s->rec_U);
+  free(s->rec_pr);
+  s->rec_max = max;
+  s->rec_n = 0;
+  s->rec_ij = (int *)calloc((size_t)2 * max, sizeof(int));
+  s->rec_U = (double *)calloc((size_t)NPR * max, sizeof(double));
+  s->rec_pr = (double *)calloc((size_t)NPR * max, sizeof(double));
+  return (s->rec_ij && s->rec_U && s->rec_pr) ? 0 : 1;
+}
+
+/* copies the recorded failures out (each array sized for max); returns
+   their number */
+int ho_get_failures(const ho_state *s, int *ij, double *U, double *pr)
+{
+  if (s->rec_n) {
+    memcpy(ij, s->rec_ij, sizeof(int) * 2 * s->rec_n);
+    memcpy(U, s->rec_U, sizeof(double) * NPR * s->rec_n);
+    memcpy(pr, s->rec_pr, sizeof(double) * NPR * s->rec_n);
+  }
+  return s->rec_n;
+}
 
 int ho_utoprim(ho_state *s, int i, int j, const double *U, double *pr)
 {

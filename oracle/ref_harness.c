@@ -112,6 +112,7 @@ int isenoughfreespace(unsigned long long need) { (void)need; return 1; }
 int init_postfield(FTYPE pr[][N2M][NPR]) { (void)pr; return 0; }
 FTYPE cot(FTYPE arg) { return 1.0 / tan(arg); }
 
+#ifndef HR_TRYAGAIN
 /* patch 7 stubs: only reachable through the disabled UTOPRIMTRYAGAIN chain */
 static int hr_unreachable(const char *who)
 {
@@ -125,6 +126,7 @@ int Utoprim_5d2_final(FTYPE U[NPR], struct of_geom *g, FTYPE prim[NPR]) { (void)
 int dudp_calc_gen(int w, FTYPE *pr, struct of_state *q, struct of_geom *g, FTYPE **alpha) { (void)w; (void)pr; (void)q; (void)g; (void)alpha; return hr_unreachable("dudp_calc_gen"); }
 FTYPE contract(FTYPE *a1, FTYPE *a2) { return a1[0]*a2[0] + a1[1]*a2[1] + a1[2]*a2[2] + a1[3]*a2[3]; }
 FTYPE covtract(FTYPE *a1, FTYPE *a2) { return a1[0]*a2[0] + a1[1]*a2[1] + a1[2]*a2[2] + a1[3]*a2[3]; }
+#endif
 
 /* ------------------------------------------------------------------ */
 /* patch 11: deterministic cycle-break factor in [0,1).
@@ -321,3 +323,26 @@ int hr_utoprimgen(int i, int j, const double *U, double *pr, int *pfl)
   *pfl = pflag[i][j][FLAGUTOPRIMFAIL];
   return 0;
 }
+
+/* one inversion by the chosen method (Utoprimgen_pick, step_ch.c:583-600,
+   `which` = UTOPRIM5D1 ... UTOPRIM5D2 of step_ch.h:39-53) of U in the
+   evolved form, as Utoprimgen feeds it (UtoU to the geometry-free form
+   first); pflag is cleared before the call */
+int hr_utoprim_pick(int which, int i, int j, const double *U, double *pr, int *pfl)
+{
+  extern void UtoU(int inputtype, int returntype, struct of_geom *ptrgeom, FTYPE *Uin, FTYPE *Uout);
+  extern int Utoprimgen_pick(int which, int parameter, FTYPE *Ugeomfree, struct of_geom *ptrgeom, FTYPE *pr);
+  struct of_geom geom;
+  FTYPE Uc[NPR], Ug[NPR], pc[NPR];
+  int k;
+  get_geometry(i, j, CENT, &geom);
+  for (k = 0; k < NPR; k++) { Uc[k] = U[k]; pc[k] = pr[k]; }
+  UtoU(UEVOLVE, UNOTHING, &geom, Uc, Ug);
+  pflag[i][j][FLAGUTOPRIMFAIL] = 0;
+  Utoprimgen_pick(which, EVOLVENOENTROPY, Ug, &geom, pc);
+  for (k = 0; k < NPR; k++) pr[k] = pc[k];
+  *pfl = pflag[i][j][FLAGUTOPRIMFAIL];
+  return 0;
+}
+
+int hr_tryagain(void) { return UTOPRIMTRYAGAIN; }

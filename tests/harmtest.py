@@ -69,6 +69,8 @@ def oracle_lib():
         lib.ho_ncyclebreak.restype = ctypes.c_long
         lib.ho_cycle_break_uniform.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int]
         lib.ho_cycle_break_uniform.restype = ctypes.c_double
+        lib.ho_record_failures.argtypes = [vp, ctypes.c_int]
+        lib.ho_get_failures.argtypes = [vp, ctypes.POINTER(ctypes.c_int), dp, dp]
         _oracle = lib
     return _oracle
 
@@ -138,6 +140,18 @@ class Oracle:
         out = np.zeros(6)
         self.lib.ho_get_horizon(self.h, _dp(out))
         return out
+
+    def record_failures(self, max_cases):
+        """records the inputs of the next max_cases failed inversions"""
+        self._rec_max = max_cases
+        assert self.lib.ho_record_failures(self.h, max_cases) == 0
+
+    def failures(self):
+        """(zones [n, 2], U [n, 8] evolved form, guesses [n, 8]) recorded"""
+        m = self._rec_max
+        ij, U, pr = np.zeros((m, 2), dtype=np.int32), np.zeros((m, 8)), np.zeros((m, 8))
+        n = self.lib.ho_get_failures(self.h, ij.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(U), _dp(pr))
+        return ij[:n].copy(), U[:n].copy(), pr[:n].copy()
 
 
 # ---------------------------------------------------------------- reference
@@ -252,6 +266,81 @@ def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=
         os.unlink(out)
 
 
+def _ref_pick_worker(libpath, methods, ij, U, pr, outpath):
+    """Runs in a child process: reference init, then Utoprimgen_pick of each
+    method on each case (zone ij, evolved U, guess pr)."""
+    import pickle
+    lib = ctypes.CDLL(libpath)
+    lib.hr_configure.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double]
+    lib.hr_configure(3, 1, 2, 0.8, 0, 1e30)
+    work = tempfile.mkdtemp(prefix="harmref_")
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved, saved1 = os.dup(2), os.dup(1)
+    os.dup2(devnull, 2)
+    os.dup2(devnull, 1)
+    try:
+        if lib.hr_init(work.encode()) != 0:
+            raise RuntimeError("reference init failed")
+        V = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        out = {}
+        for m in methods:
+            prs = np.zeros_like(pr)
+            codes = np.zeros(len(ij), dtype=np.int32)
+            for c in range(len(ij)):
+                pc = pr[c].copy()
+                pf = ctypes.c_int(0)
+                lib.hr_utoprim_pick(int(m), int(ij[c, 0]), int(ij[c, 1]), V(np.ascontiguousarray(U[c])), V(pc),
+                                    ctypes.byref(pf))
+                prs[c] = pc
+                codes[c] = pf.value
+            out[int(m)] = (prs, codes)
+        chain_pr = np.zeros_like(pr)
+        chain_codes = np.zeros(len(ij), dtype=np.int32)
+        lib.hr_utoprimgen.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        for c in range(len(ij)):
+            pc = pr[c].copy()
+            pf = ctypes.c_int(0)
+            lib.hr_utoprimgen(int(ij[c, 0]), int(ij[c, 1]), V(np.ascontiguousarray(U[c])), V(pc), ctypes.byref(pf))
+            chain_pr[c] = pc
+            chain_codes[c] = pf.value
+        out["chain"] = (chain_pr, chain_codes)
+    finally:
+        os.dup2(saved, 2)
+        os.dup2(saved1, 1)
+    with open(outpath, "wb") as f:
+        pickle.dump(out, f, protocol=4)
+
+
+def ref_utoprim_pick(n1, n2, methods, ij, U, pr, problem="torusta", timeout=1800):
+    """Each method of the retry chain (Utoprimgen_pick, step_ch.h:39-53 ids)
+    and the whole Utoprimgen (the chain itself in the torusta build) of the
+    compiled reference on the given cases: {method: (pr, pflag)} plus
+    "chain".  None when that build is absent."""
+    import pickle
+    import sys
+    path = ref_lib_path(n1, n2, problem)
+    if path is None:
+        return None
+    fd, out = tempfile.mkstemp(suffix=".pkl", prefix="harmref_")
+    os.close(fd)
+    fi, inp = tempfile.mkstemp(suffix=".npz", prefix="harmref_")
+    os.close(fi)
+    np.savez(inp, ij=ij, U=U, pr=pr)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import harmtest; d = np.load(%r); "
+            "harmtest._ref_pick_worker(%r, %r, d['ij'], d['U'], d['pr'], %r)"
+            % (os.path.dirname(os.path.abspath(__file__)), inp, path, list(methods), out))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed (rc=%d): %s" % (r.returncode, r.stderr[-2000:]))
+        with open(out, "rb") as f:
+            return pickle.load(f)
+    finally:
+        os.unlink(out)
+        os.unlink(inp)
+
+
 def ref_config(r):
     """harm config keyword arguments from a reference run's scalars."""
     s = r["scalars"]
@@ -261,3 +350,38 @@ def ref_config(r):
 
 def interior(a):
     return a[NG:-NG, NG:-NG]
+
+
+# ---------------------------------------------------------------- retry chain
+TA_HOST_SRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tryagain_host.cu")
+TA_HOST_LIB = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "libtryagain_host.so")
+TA_HDRS = [os.path.join(ROOT, "harm_ramt_b200", "csrc", f) for f in ("harm_tryagain.cuh", "harm_device.cuh")]
+
+
+def tryagain_host_lib():
+    """The retry chain's inversions (harm_tryagain.cuh) compiled for the CPU
+    (tests/tryagain_host.cu), or None without nvcc."""
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        return None
+    deps = [TA_HOST_SRC] + TA_HDRS
+    if not os.path.exists(TA_HOST_LIB) or any(os.path.getmtime(d) > os.path.getmtime(TA_HOST_LIB) for d in deps):
+        os.makedirs(os.path.dirname(TA_HOST_LIB), exist_ok=True)
+        subprocess.run([nvcc, "-O2", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o",
+                        TA_HOST_LIB + ".tmp", TA_HOST_SRC], check=True, capture_output=True)
+        os.replace(TA_HOST_LIB + ".tmp", TA_HOST_LIB)
+    lib = ctypes.CDLL(TA_HOST_LIB)
+    P = ctypes.POINTER(ctypes.c_double)
+    d = ctypes.c_double
+    lib.ta_pick.argtypes = [ctypes.c_int, P, P, d, d, d, P, P]
+    lib.ta_chain.argtypes = [P, P, d, d, d, P, P, P, ctypes.c_int]
+    lib.ta_primtoU.argtypes = [P, P, d, d, P, P]
+    lib.ta_primtoU.restype = None
+    return lib
+
+
+def cent_geometry(geom, i, j):
+    """(gcov 4x4, gcon 4x4, sqrt(-g)) at the zone centre (i, j)"""
+    return (np.ascontiguousarray(geom["gcov"][i + NG, j + NG, 3]), np.ascontiguousarray(geom["gcon"][i + NG, j + NG, 3]),
+            float(geom["gdet"][i + NG, j + NG, 3]))
