@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--adjoint-ckpt", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=0,
                     help="if > 0, the adjoint leg runs this many steps instead of running to --adjoint-t")
+    ap.add_argument("--no-rows", action="store_true",
+                    help="skip the measurements of the retry chain, the currents and the dump writer")
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
@@ -325,6 +327,9 @@ def b200_arm(a):
     adj = None
     if a.adjoint_n > 0:
         adj = adjoint_leg(a, hb, dist)
+    rows = None
+    if not a.no_rows:
+        rows = rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist)
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -349,13 +354,82 @@ def b200_arm(a):
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
-                "ensemble": ens, "adjoint": adj,
+                "ensemble": ens, "adjoint": adj, "rows": rows,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist):
+    """The step's optional parts on the benchmark torus (device time, CUDA
+    events, max over ranks): (1) the diagnostic currents every step
+    (currents = 1) against the plain step (ms_step) in the developed flow;
+    (2) the UTOPRIMTRYAGAIN retry chain (tryagain = 1) against the 2D
+    inversion alone over the first steps from init, where the start-up
+    transient fails inversions; (3) the reference-layout dump file written
+    from the device state."""
+    import tempfile
+
+    import torch
+    n = a.n
+
+    def timed(h, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.step_ch(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / k
+
+    out = {}
+    # (1) currents, developed flow
+    h, geom, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, currents=True)
+    h.step_ch(a.evolve + a.warmup)
+    h.sync()
+    k = max(20, min(a.steps, 200))
+    ms_cur = timed(h, k)
+    h.sync()
+    out["currents"] = {"ms_per_step": ms_cur, "ms_per_step_without": ms_step, "overhead": ms_cur / ms_step - 1.0,
+                       "steps": k, "what": "Faraday slots and J^mu after every step (step_ch.c:143-156)"}
+    # (3) dump file of that state (needs the currents)
+    header, coords = hb.torus_dump_coords(hb.torus_params(n, n))
+    fd, path = tempfile.mkstemp(prefix="harm_dump_")
+    os.close(fd)
+    try:
+        h.write_dump(path, header, coords)  # first call: buffers
+        t0 = time.perf_counter()
+        h.write_dump(path, header, coords)
+        dt_dump = time.perf_counter() - t0
+        size = os.path.getsize(path)
+    finally:
+        os.unlink(path)
+    h.close()
+    out["dump"] = {"seconds": max_over_ranks(dt_dump, dist, "cuda"), "bytes": size,
+                   "MB_per_s": size / 1e6 / dt_dump,
+                   "what": "reference dump file (dump.c layout, text) of the 512^2 state from the device"}
+    # (2) retry chain over the start-up transient
+    ks = 40
+    res = {}
+    for name, ta in (("with_chain", True), ("without_chain", False)):
+        h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, tryagain=ta)
+        h.step_ch(1)  # the graph
+        h.sync()
+        res[name] = timed(h, ks)
+        st = h.sync()
+        res[name + "_fixups"] = st["fixups"]
+        h.close()
+    out["tryagain"] = {"ms_per_step": res["with_chain"], "ms_per_step_without": res["without_chain"],
+                       "steps": ks, "state": "steps 2-41 from init",
+                       "repaired_zones": {"with_chain": res["with_chain_fixups"],
+                                          "without_chain": res["without_chain_fixups"]},
+                       "what": "failed 2D inversions retried by 5D1, 2D, 1D, 1D_OPT, 1D_FINAL, 2D_FINAL, 5D2_FINAL "
+                               "(step_ch.c:608-626) before fixup_utoprim repairs the rest"}
+    return out
 
 
 def adjoint_leg(a, hb, dist):

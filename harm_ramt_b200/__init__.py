@@ -501,7 +501,7 @@ def torus_dump_coords(params):
 
 
 def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, precision=PREC_FP64, tf=1.0e30,
-                  stream=None, **torus_kw):
+                  stream=None, currents=False, tryagain=False, **torus_kw):
     """Builds the benchmark torus on the host and returns (HarmGPU, geometry,
     initial prims) with the state uploaded, bounded and t=0, dt=1e-5 set as
     init_defglobal() leaves them (initbase.c:158)."""
@@ -509,9 +509,10 @@ def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, 
     geom = torus_geometry(par)
     p0 = torus_init(par, geom)
     h = HarmGPU(n1, n2, geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, cour=cour, gam=par.gam,
-                gammamax=par.gammamax, precision=precision, tf=tf, stream=stream)
+                gammamax=par.gammamax, precision=precision, tf=tf, stream=stream, currents=currents,
+                tryagain=tryagain)
     h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
     h.set_prims(p0)
     h.bound_prims()
-    h.set_time(0.0, 1.0e-5, 0)
+    h.set_time(0.0, 1.0e-5, 0)  # with currents, also their t = 0 evaluation
     return h, geom, p0
