@@ -153,16 +153,18 @@ static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", 
                                                "k_current"};
 
 struct Timer {
-  // records an event after every launch when active
+  // records an event after every launch (or pair of launches) when active
   cudaEvent_t ev[64];
   int cls[64];
+  int nk[64];  // kernels launched since the previous event
   int n = 0;
   bool on = false;
-  void mark(cudaStream_t s, int k)
+  void mark(cudaStream_t s, int k, int kernels = 1)
   {
     if (!on || n >= 63) return;
     cudaEventRecord(ev[n + 1], s);
     cls[n + 1] = k;
+    nk[n + 1] = kernels;
     n++;
   }
 };
@@ -224,7 +226,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
     T.mark(s, KC_EMF);
     launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, pi, pb, pf, c2);
-    T.mark(s, KC_UPDATE);
+    T.mark(s, KC_UPDATE, ffde ? 1 : 2);  // k_update and k_update_tail
     if (rec) {
       cudaMemcpyAsync(rec->upd[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
       cudaMemcpyAsync(rec->flaginv[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
@@ -274,7 +276,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     T.mark(s, KC_FARADAY);
     k_current<<<grid2(n1 + 2 * NG - 2, n2 + 2 * NG - 2, b), b, 0, s>>>(a);
     k_currents_commit<<<1, 1, 0, s>>>(a);
-    T.mark(s, KC_CURRENT);
+    T.mark(s, KC_CURRENT, 2);
   }
   launch_horizon(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
   T.mark(s, KC_HORIZON);
@@ -1235,7 +1237,7 @@ int harm_profile_step(harm_ctx* c, double* ms, int* launches, int nclasses)
     float t = 0.f;
     cudaEventElapsedTime(&t, T.ev[k - 1], T.ev[k]);
     ms[T.cls[k]] += t;
-    launches[T.cls[k]] += 1;
+    launches[T.cls[k]] += T.nk[k];
   }
   for (int k = 0; k < 64; k++) cudaEventDestroy(T.ev[k]);
   return rc;
