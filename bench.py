@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--adjoint-ckpt", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=0,
                     help="if > 0, the adjoint leg runs this many steps instead of running to --adjoint-t")
+    ap.add_argument("--sizes", default="512,1024",
+                    help="grid sizes of the HLL/LAXF side measurements (empty: skip them)")
     ap.add_argument("--no-rows", action="store_true",
                     help="skip the measurements of the retry chain, the currents and the dump writer")
     ap.add_argument("--ref-budget", type=float, default=100.0,
@@ -330,6 +332,9 @@ def b200_arm(a):
     rows = None
     if not a.no_rows:
         rows = rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist)
+    sizes = None
+    if a.sizes:
+        sizes = sizes_leg(a, hb, stream, lim, barrier, dist)
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -354,13 +359,43 @@ def b200_arm(a):
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
-                "ensemble": ens, "adjoint": adj, "rows": rows,
+                "ensemble": ens, "adjoint": adj, "rows": rows, "sizes": sizes,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def sizes_leg(a, hb, stream, lim, barrier, dist):
+    """The same torus at the other grid sizes and with the other Riemann
+    solver (HLL and LAXF at each size in --sizes): whole-job zone-cycles/s
+    after 100 untimed steps, device time of 100 steps (max over ranks)."""
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    out = {}
+    for n in [int(s) for s in a.sizes.split(",") if s]:
+        for fname, fl in (("hll", hb.FLUX_HLL), ("laxf", hb.FLUX_LAXF)):
+            if n == a.n and fl == (hb.FLUX_HLL if a.flux == "hll" else hb.FLUX_LAXF):
+                continue  # the headline line itself
+            h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=fl, stream=stream.cuda_stream)
+            h.step_ch(100)
+            h.sync()
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.step_ch(100)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / 100
+            h.sync()
+            h.close()
+            out[f"{n}_{fname}"] = {"value": aggregate_rate(world, n * n, ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                                   "workload": f"{n}x{n} torus, FP64, {a.lim.upper()} + {fname.upper()}, "
+                                               "steps 101-200 from init"}
+    return out
 
 
 def rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist):
