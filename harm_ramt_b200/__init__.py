@@ -78,7 +78,7 @@ class _Tiles(ctypes.Structure):
 class _Status(ctypes.Structure):
     _fields_ = [("fail_code", ctypes.c_int), ("fail_i", ctypes.c_int), ("fail_j", ctypes.c_int),
                 ("fixups", ctypes.c_int), ("realnstep", ctypes.c_longlong), ("t", ctypes.c_double),
-                ("dt", ctypes.c_double), ("newton_iters", ctypes.c_ulonglong)]
+                ("dt", ctypes.c_double), ("newton_iters", ctypes.c_ulonglong), ("chk_multi", ctypes.c_int)]
 
 
 class _TorusParams(ctypes.Structure):
@@ -356,7 +356,7 @@ class HarmGPU:
         st = _Status()
         rc = self.lib.harm_sync(self._h, ctypes.byref(st))
         d = dict(fail_code=st.fail_code, fail_i=st.fail_i, fail_j=st.fail_j, fixups=st.fixups,
-                 realnstep=st.realnstep, t=st.t, dt=st.dt, newton_iters=st.newton_iters)
+                 realnstep=st.realnstep, t=st.t, dt=st.dt, newton_iters=st.newton_iters, chk_multi=st.chk_multi)
         if rc == 6 and raise_on_fail:
             raise HarmError(rc, f"step failed with {FAIL_NAMES.get(st.fail_code, st.fail_code)} at zone "
                                 f"({st.fail_i},{st.fail_j})")

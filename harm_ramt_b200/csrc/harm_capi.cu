@@ -622,6 +622,7 @@ int harm_sync(harm_ctx* c, harm_status* st)
     st->t = h.t;
     st->dt = h.dt;
     st->newton_iters = h.newton_iters;
+    st->chk_multi = h.chk_multi;
   }
   return h.status ? HARM_EFAIL : HARM_OK;
 }

@@ -60,6 +60,7 @@ struct DevScalars {
   int cur_ring;          // currents: ring level holding the newest F^{i t}
   long long ccalls;      // currents: calls of current_calc_1 (its static count)
   double clastdt;        // currents: dt of the previous call (its static lastdt)
+  int chk_multi;         // substeps whose check-solution sweep ran more than one round
 };
 
 struct StepArgs {

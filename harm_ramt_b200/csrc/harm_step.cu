@@ -323,7 +323,10 @@ __global__ void k_checksol(StepArgs a, const double* __restrict__ pv, int round)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (round > 0 && !a.sc->chk_changed[round - 1]) return;
-  if (i == 0 && j == 0) a.sc->chk_final = round;
+  if (i == 0 && j == 0) {
+    a.sc->chk_final = round;
+    if (round == 1) a.sc->chk_multi++;
+  }
   if (i >= a.gr.n1 || j >= a.gr.n2) return;
   const long long z = a.gr.at(i, j), pl = a.gr.plane;
   unsigned char* cur = a.chk + (long long)(round & 1) * pl;

@@ -107,6 +107,9 @@ typedef struct harm_status {
   long long realnstep;
   double t, dt;                  /* time and the next step's dt */
   unsigned long long newton_iters; /* Newton iterations since harm_set_time */
+  int chk_multi;                 /* substeps since harm_set_time whose check-solution
+                                    sweep (fixup.c:388-488) needed more than one
+                                    parallel round */
 } harm_status;
 
 typedef struct harm_ctx harm_ctx;
