@@ -46,7 +46,7 @@ def test_graph_step_matches_unconditional_launches(harm, n, lim, flux, nsteps):
 TEST_COUNTS = {}
 
 
-def test_conditional_body_was_exercised():
+def test_multi_round_sweeps_were_exercised():
     if len(TEST_COUNTS) < 2:
         pytest.skip("the comparison runs did not complete")
     assert sum(TEST_COUNTS.values()) > 0, f"no multi-round sweep in the runs: {TEST_COUNTS}"
