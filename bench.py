@@ -30,7 +30,10 @@ import numpy as np  # noqa: E402
 
 METRIC = "zone-cycles/s, 512² torus"
 UNIT = "zone-cycles/s"
-BYTES_PER_ZONE_CYCLE = 2032  # algorithmic FP64 bytes per zone-cycle
+# algorithmic FP64 bytes per zone-cycle of the whole step: two substeps of
+# k_flux (528 B/zone) and k_update (836 B/zone), the EMF and b^2-flag passes
+# and the small fixup/boundary kernels' reads of the state
+BYTES_PER_ZONE_CYCLE = 2032
 
 
 def parse():
@@ -654,7 +657,8 @@ def mixed_precision_leg(a, hb, stream, lim, flux, value_fp64, barrier, dist):
     return out
 
 
-# algorithmic bytes per active zone of one launch (FP64)
+# algorithmic bytes per active zone of one launch (FP64): every plane each
+# kernel must read or write once, 8 bytes a value
 KERNEL_BYTES = {
     "k_flux": 8 * (8 + 2 * 21 + 2 * 8),       # prims once, FACE1+FACE2 geometry, F1+F2 out
     "k_update": 8 * (8 + 8 + 21 + 40 + 2 + 2 * 8 + 1 + 8) + 4,  # pi, pb, CENT geo, conn, floors, 2 faces x2, emf, pf, pflag
