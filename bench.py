@@ -30,9 +30,11 @@ import numpy as np  # noqa: E402
 
 METRIC = "zone-cycles/s, 512² torus"
 UNIT = "zone-cycles/s"
-# algorithmic FP64 bytes per zone-cycle of the whole step: two substeps of
-# k_flux (528 B/zone) and k_update (836 B/zone), the EMF and b^2-flag passes
-# and the small fixup/boundary kernels' reads of the state
+# algorithmic FP64 bytes per zone-cycle of the whole step, each value moved
+# once: the state read and written (p in, pk out; pk and p in, p out: 5 x 64
+# B), per substep the geometry (CENT, FACE1, FACE2 metric and sqrt(-g), CORN
+# sqrt(-g), the 40 connection coefficients: 832 B), the floors (16 B) and
+# the pflag read and write (8 B)
 BYTES_PER_ZONE_CYCLE = 2032
 
 
