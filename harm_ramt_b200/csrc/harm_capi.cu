@@ -331,7 +331,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   c->gr.plane = (long long)c->gr.pitch * c->gr.rows;
   const size_t pd = (size_t)c->gr.plane * sizeof(double);
   const dim3 b(32, 4);
-  c->flux_by = flux_rows(cfg->n1, cfg->n2);
+  c->flux_by = flux_rows(cfg->n1, cfg->n2, cfg->precision == HARM_PREC_MIXED);
   dim3 gf = flux_grid(cfg->n1, cfg->n2, c->flux_by);
   c->nblocks_flux = gf.x * gf.y;
   c->tile_update = dim3(32, 4);
@@ -1347,7 +1347,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.gr.rows = c.n2m;
   c.gr.plane = (long long)c.gr.pitch * c.gr.rows;
   const dim3 b(32, 4);
-  c.flux_by = flux_rows(cfg->n1, cfg->n2);
+  c.flux_by = flux_rows(cfg->n1, cfg->n2, false);
   const dim3 gf = flux_grid(cfg->n1, cfg->n2, c.flux_by);
   c.nblocks_flux = gf.x * gf.y;
   c.tile_update = dim3(32, 4);

@@ -140,11 +140,14 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 // without recomputing a neighbour's interface state.  16 rows leave less
 // x2 recomputation (one row in 16) but hold one 512-thread block per SM:
 // they are used when that grid still fills three waves of the 148 SMs,
-// 4 rows (four 128-thread blocks per SM) on smaller grids.
+// 4 rows (four 128-thread blocks per SM) on smaller grids.  The FP32 faces
+// of the mixed form fit 128 registers without spilling and run best as
+// 4-row blocks at four per SM on any grid.
 constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = 16;
 inline dim3 flux_grid(int n1, int n2, int by) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + by - 1) / by); }
-inline int flux_rows(int n1, int n2)
+inline int flux_rows(int n1, int n2, bool fp32_faces)
 {
+  if (fp32_faces) return FLUX_BY_SMALL;
   const dim3 g = flux_grid(n1, n2, FLUX_BY_LARGE);
   return (g.x * g.y >= 3 * 148) ? FLUX_BY_LARGE : FLUX_BY_SMALL;
 }

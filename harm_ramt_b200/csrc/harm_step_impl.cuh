@@ -119,10 +119,10 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // FLUX_BX = 31 along x1): lane 0 only lends its right state, and its faces
 // are the previous block's (block 0's lane 0 is zone -1, which has no x1
 // face but an x2 face).
-// BY = 4 or 16 rows per block (flux_rows).  FP64 faces: at most 128
-// registers a thread either way (512 threads per SM).
+// BY = 4 or 16 rows per block (flux_rows).  At most 128 registers a thread:
+// 512 threads per SM for the FP64 faces, four 4-row blocks for the FP32 ones.
 template <typename T, bool PARA, bool FFDE, int BY>
-__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 1) k_flux(StepArgs a, const double* __restrict__ pb)
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 4 : 1)) k_flux(StepArgs a, const double* __restrict__ pb)
 {
   __shared__ double sh[2][32];
   __shared__ T shr[NPR][BY][32];
