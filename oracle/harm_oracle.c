@@ -22,6 +22,12 @@
  * (bounds.fishmon.c: OUTFLOW at both x1 ends, polar mirror with POLEDEATH)
  * or the rotating star's (bounds.ns.c: NSSURFACE inside, extrapolating
  * OUTFLOW outside, plain polar mirror).
+ *
+ * The UTOPRIMTRYAGAIN retry chain (step_ch.c:608-626) is not restated here:
+ * its inversion methods are pinned directly against the reference built
+ * with the chain on (oracle/build_ref.py --problem torusta).  This file
+ * supplies their test inputs: ho_record_failures()/ho_get_failures() keep
+ * the zone, U and guess of every 2D inversion that fails.
  */
 #include "harm_oracle.h"
 

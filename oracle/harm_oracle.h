@@ -73,6 +73,14 @@ long ho_ncyclebreak(const ho_state *s);
 /* single-zone inversion of an evolved U (with sqrt(-g)) at zone (i,j) */
 int ho_utoprim(ho_state *s, int i, int j, const double *U, double *pr);
 
+/* from now on, record the zone, evolved U and guess of up to max failed 2D
+   inversions of the steps (inputs for the retry chain's tests) */
+int ho_record_failures(ho_state *s, int max);
+
+/* copies the recorded failures out (ij: 2 ints, U and pr: 8 doubles each per
+   failure; arrays sized for the max given); returns their number */
+int ho_get_failures(const ho_state *s, int *ij, double *U, double *pr);
+
 /* the deterministic cycle-break factor (shared with the GPU kernel) */
 double ho_cycle_break_uniform(double x0, double x1, int n_iter);
 
