@@ -22,7 +22,6 @@ enum { M_5D1 = 0, M_LDZ = 1, M_2D = 2, M_1D = 3, M_1DOPT = 4, M_1DFINAL = 5, M_2
 constexpr int PF_CONV = 1;  // UTOPRIMFAILCONV, global.h:550
 
 HD_INLINE double gcov_at(const Geo<double>& g, int j, int k) { return g.gcov[sym(j, k)]; }
-HD_INLINE double gcon_at(const Geo<double>& g, int j, int k) { return g.gcon[sym(j, k)]; }
 HD_INLINE double kdelta(int a, int b) { return (a == b) ? 1.0 : 0.0; }
 
 // primtoU(UNOTHING), phys.c:16-56 and 219-265 (dir 0, no sqrt(-g), T^t_t
