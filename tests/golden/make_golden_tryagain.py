@@ -32,7 +32,7 @@ METHODS = (0, 2, 3, 4, 5, 6, 7)
 OUT = os.path.join(HERE, "tryagain32.npz")
 
 
-def cases():
+def cases(seed=20261203, nsynth=240):
     par = hb.torus_params(N, N)
     geom = hb.torus_geometry(par)
     p0 = hb.torus_init(par, geom)
@@ -50,9 +50,9 @@ def cases():
         assert rc == 0
     lib = ht.tryagain_host_lib()
     P = ctypes.POINTER(ctypes.c_double)
-    rng = np.random.default_rng(20261203)
+    rng = np.random.default_rng(seed)
     ij, U, pr = [], [], []
-    for c in range(240):
+    for c in range(nsynth):
         i, j = int(rng.integers(0, N)), int(rng.integers(0, N))
         p = po[i + ht.NG, j + ht.NG].copy()
         gc, gn, gd = ht.cent_geometry(geom, i, j)

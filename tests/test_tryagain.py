@@ -101,3 +101,31 @@ def test_fixture_is_the_reference(fix):
         assert np.array_equal(ref[m][1], fix[f"code_{m}"]) and np.array_equal(ref[m][0], fix[f"pr_{m}"], equal_nan=True)
     assert np.array_equal(ref["chain"][1], fix["chain_code"])
     assert np.array_equal(ref["chain"][0], fix["chain_pr"], equal_nan=True)
+
+
+@pytest.mark.parametrize("seed", [11, 47])
+def test_methods_match_reference_on_fresh_cases(geom, host, seed):
+    """the same comparison on cases drawn afresh (another seed of the fixture
+    generator's perturbations), against the reference run now"""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden_tryagain as mg
+    ij, U, pr, _ = mg.cases(seed=seed, nsynth=200)
+    ref = ht.ref_utoprim_pick(N, N, (0, 2, 3, 4, 5, 6, 7), ij, U, pr)
+    if ref is None:
+        pytest.skip("reference build with the retry chain (oracle/_ref) not present")
+    for m in (0, 3, 4, 5, 6, 7):
+        rpr, rcode = ref[m]
+        for c, (i, j) in enumerate(ij):
+            gc, gn, gd = ht.cent_geometry(geom, int(i), int(j))
+            x = pr[c].copy()
+            code = host.ta_pick(m, _p(gc), _p(gn), gd, GAM, GAMMAFAIL, _p(np.ascontiguousarray(U[c])), _p(x))
+            assert code == rcode[c] and np.array_equal(x, rpr[c], equal_nan=True), f"seed {seed} method {m} case {c}"
+    rpr, rcode = ref["chain"]
+    for c, (i, j) in enumerate(ij):
+        gc, gn, gd = ht.cent_geometry(geom, int(i), int(j))
+        x = ref[2][0][c].copy()
+        code = host.ta_chain(_p(gc), _p(gn), gd, GAM, GAMMAFAIL, _p(np.ascontiguousarray(U[c])),
+                             _p(np.ascontiguousarray(pr[c])), _p(x), int(ref[2][1][c]))
+        assert code == rcode[c] and np.array_equal(x, rpr[c], equal_nan=True), f"seed {seed} chain case {c}"
+
