@@ -78,7 +78,8 @@ class _Tiles(ctypes.Structure):
 class _Status(ctypes.Structure):
     _fields_ = [("fail_code", ctypes.c_int), ("fail_i", ctypes.c_int), ("fail_j", ctypes.c_int),
                 ("fixups", ctypes.c_int), ("realnstep", ctypes.c_longlong), ("t", ctypes.c_double),
-                ("dt", ctypes.c_double), ("newton_iters", ctypes.c_ulonglong), ("chk_multi", ctypes.c_int)]
+                ("dt", ctypes.c_double), ("newton_iters", ctypes.c_ulonglong), ("chk_multi", ctypes.c_int),
+                ("deferred", ctypes.c_int), ("fail_step", ctypes.c_longlong)]
 
 
 class _TorusParams(ctypes.Structure):
@@ -356,7 +357,8 @@ class HarmGPU:
         st = _Status()
         rc = self.lib.harm_sync(self._h, ctypes.byref(st))
         d = dict(fail_code=st.fail_code, fail_i=st.fail_i, fail_j=st.fail_j, fixups=st.fixups,
-                 realnstep=st.realnstep, t=st.t, dt=st.dt, newton_iters=st.newton_iters, chk_multi=st.chk_multi)
+                 realnstep=st.realnstep, t=st.t, dt=st.dt, newton_iters=st.newton_iters, chk_multi=st.chk_multi,
+                 deferred=st.deferred, fail_step=st.fail_step)
         if rc == 6 and raise_on_fail:
             raise HarmError(rc, f"step failed with {FAIL_NAMES.get(st.fail_code, st.fail_code)} at zone "
                                 f"({st.fail_i},{st.fail_j})")
@@ -474,7 +476,8 @@ class Ensemble:
         st = (_Status * len(self.members))()
         rc = self.lib.harm_ensemble_sync(self._h, st)
         out = [dict(fail_code=s.fail_code, fail_i=s.fail_i, fail_j=s.fail_j, fixups=s.fixups, realnstep=s.realnstep,
-                    t=s.t, dt=s.dt, newton_iters=s.newton_iters) for s in st]
+                    t=s.t, dt=s.dt, newton_iters=s.newton_iters, deferred=s.deferred, fail_step=s.fail_step)
+               for s in st]
         if rc == 6 and raise_on_fail:
             bad = [k for k, s in enumerate(out) if s["fail_code"]]
             raise HarmError(rc, f"ensemble members {bad} failed")

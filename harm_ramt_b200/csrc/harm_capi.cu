@@ -214,6 +214,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
       a.rec_fixset = rec->fixset[sub];
     }
     a.bsqf_fused = (fuse_bsq && sub == 0) ? a0.bsqf : nullptr;
+    a.phase0 = sub * PH_PER_SUBSTEP;
     const double* pi = c->d_p;
     const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
@@ -607,24 +608,47 @@ int harm_step(harm_ctx* c, int nsteps)
   return HARM_OK;
 }
 
+// the run state of the device scalars; the first fatal check is decoded
+// from its key (fail_key: step, phase, position in the phase's loop, code)
+static void fill_status(const DevScalars& h, int n1, int n2, harm_status* st)
+{
+  if (!st) return;
+  const unsigned long long key = ~h.fail_inv;
+  st->fail_code = 0;
+  st->fail_i = st->fail_j = 0;
+  st->fail_step = -1;
+  if (h.fail_inv) {
+    const int phase = (int)((key >> 36) & 15) % PH_PER_SUBSTEP;
+    const unsigned o = (unsigned)((key >> 6) & 0x3fffffffu);
+    st->fail_code = (int)(key & 63);
+    st->fail_step = (long long)(key >> 40);
+    if (phase == PH_BOUND1 || phase == PH_BOUND2) {
+      const bool outer = o >= (unsigned)(n2 * NG);
+      const unsigned r = outer ? o - (unsigned)(n2 * NG) : o;
+      st->fail_j = (int)(r / NG);
+      st->fail_i = outer ? n1 + (int)(r % NG) : -1 - (int)(r % NG);
+    } else {
+      st->fail_i = (int)(o >> 15) - NG;
+      st->fail_j = (int)(o & 0x7fff) - NG;
+    }
+  }
+  st->fixups = h.fixups;
+  st->realnstep = h.realnstep;
+  st->t = h.t;
+  st->dt = h.dt;
+  st->newton_iters = h.newton_iters;
+  st->chk_multi = h.chk_multi;
+  st->deferred = h.ndeferred_total;
+}
+
 int harm_sync(harm_ctx* c, harm_status* st)
 {
   if (!c) return HARM_EINVAL;
   DevScalars h;
   CK(cudaMemcpyAsync(&h, c->d_sc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (st) {
-    st->fail_code = h.status;
-    st->fail_i = h.status ? (h.status_zone % 100000) - NG : 0;
-    st->fail_j = h.status ? (h.status_zone / 100000) - NG : 0;
-    st->fixups = h.fixups;
-    st->realnstep = h.realnstep;
-    st->t = h.t;
-    st->dt = h.dt;
-    st->newton_iters = h.newton_iters;
-    st->chk_multi = h.chk_multi;
-  }
-  return h.status ? HARM_EFAIL : HARM_OK;
+  fill_status(h, c->cfg.n1, c->cfg.n2, st);
+  return h.fail_inv ? HARM_EFAIL : HARM_OK;
 }
 
 int harm_get_currents(harm_ctx* c, double* jcon, double* fcon, double* cfaraday)
@@ -1402,5 +1426,5 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   CK(cudaStreamSynchronize(c.stream));
   *t = h.t;
   *dt = h.dt;
-  return h.status ? HARM_EFAIL : HARM_OK;
+  return h.fail_inv ? HARM_EFAIL : HARM_OK;
 }

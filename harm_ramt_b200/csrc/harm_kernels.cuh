@@ -47,8 +47,7 @@ struct DevScalars {
   double t, dt, ndt;
   double dt_free;        // the next dt before the end-time clamp
   long long realnstep;
-  int status;            // first fatal fail code (0 = ok)
-  int status_zone;       // i + (n1+6)*j of the first failure (+ offsets)
+  unsigned long long fail_inv;  // ~key of the first fatal check in the reference's order (0 = none; see fail_key)
   unsigned long long newton_iters;   // Newton iterations since the last reset
   int chk_changed[8];    // per-round change flags of the check-solution sweep
   int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
@@ -85,6 +84,7 @@ struct StepArgs {
   double* rec_pinv;      // adjoint recording (or null): inverted prims before the floors, 8 planes
   unsigned char* rec_fixset;  // adjoint recording (or null): neighbour set of each repaired zone
   int nblocks_flux;
+  int phase0;            // PH_PER_SUBSTEP * substep: the fail-key phase of this launch's substep
   DevScalars* sc;
 };
 
@@ -103,9 +103,33 @@ __device__ __forceinline__ unsigned char bsq_flag(const StepArgs& a, const doubl
   return (unsigned char)(f0 | (f3 << 2));
 }
 
-__device__ __forceinline__ void report_fail(DevScalars* sc, int code, int i, int j)
+// Phases of a substep in the order the reference runs them; a fatal check
+// ends the reference's step at the first zone of the first phase in loop
+// order (fail(), fail.c:4-57, then every caller returns), so the device
+// keeps the smallest key over all reports -- (step, substep phase, position
+// of the zone in that phase's loop, code) -- and the reported zone and code
+// are those of the reference whatever the order in which threads reach them.
+enum { PH_FACE1 = 0, PH_FACE2 = 1, PH_UPDATE = 2, PH_BOUND1 = 3, PH_FIXUP = 4, PH_BOUND2 = 5, PH_PER_SUBSTEP = 8 };
+// position in ZLOOP / FZLOOP order (i outer, j inner)
+__host__ __device__ __forceinline__ unsigned zone_order(int i, int j)
 {
-  if (atomicCAS(&sc->status, 0, code) == 0) sc->status_zone = (i + NG) + 100000 * (j + NG);
+  return ((unsigned)((i + NG) & 0x7fff) << 15) | (unsigned)((j + NG) & 0x7fff);
+}
+// position in bound_prim's x1 ghost loops (bounds.fishmon.c:30-110, 113-200):
+// the inner ghosts first (j outer, i = -1, -2, -3), then the outer ones
+__host__ __device__ __forceinline__ unsigned bound_order(int n1, int n2, int i, int j)
+{
+  return (i < 0) ? (unsigned)(j * NG + (-1 - i)) : (unsigned)(n2 * NG + j * NG + (i - n1));
+}
+__host__ __device__ __forceinline__ unsigned long long fail_key(long long step, int phase, unsigned order, int code)
+{
+  const unsigned long long st = (step < 0) ? 0ULL : ((step > 0xffffffLL) ? 0xffffffULL : (unsigned long long)step);
+  return (st << 40) | ((unsigned long long)(phase & 15) << 36) | ((unsigned long long)(order & 0x3fffffffu) << 6) |
+         (unsigned long long)(code & 63);
+}
+__device__ __forceinline__ void report_fail(DevScalars* sc, int phase, int code, unsigned order)
+{
+  atomicMax(&sc->fail_inv, ~fail_key(sc->realnstep, phase, order, code));
 }
 
 // FP32 copy of a face location's geometry (mixed precision)

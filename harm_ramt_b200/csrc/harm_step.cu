@@ -212,7 +212,7 @@ __device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* p
 
 // outflow copy + inflow check + gamma limit of an x1 ghost zone (i, j),
 // bounds.fishmon.c:28-60 and 192-230 (EXTRAP 0), or the star's
-__device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, int i, int j, double* pr)
+__device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, int i, int j, double* pr, int phase)
 {
   if (a.pp.bc == 1) {
     x1_ghost_star(a, pv, i, j, pr);
@@ -226,7 +226,7 @@ __device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, in
   load_geo(a, CENT, a.gr.at(i, j), g);
   int rc = inflow_check_x1(a, i, pr, g);
   if (!rc) rc = limit_gamma(a.pp.gammamax, pr, g);
-  if (rc) report_fail(a.sc, rc, i, j);
+  if (rc) report_fail(a.sc, phase, rc, bound_order(a.gr.n1, a.gr.n2, i, j));
 }
 
 // bound_prim (bounds.fishmon.c:14-330 or bounds.ns.c:10-355) and
@@ -246,8 +246,9 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
   double pr[NPR];
   const bool poledeath = (a.pp.bc == 0);
+  const int phase = a.phase0 + (with_pflag ? PH_BOUND1 : PH_BOUND2);
   if (yin) {
-    x1_ghost(a, pv, i, j, pr);
+    x1_ghost(a, pv, i, j, pr, phase);
     if (poledeath && (j == 0 || j == n2 - 1)) {
       pr[U2] *= 0.;
       pr[B2] *= 0.;
@@ -259,7 +260,7 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
 #pragma unroll
       for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + zs];
     } else {
-      x1_ghost(a, pv, i, jm, pr);
+      x1_ghost(a, pv, i, jm, pr, phase);
     }
     if (poledeath) {
       pr[U2] *= 0.;
@@ -488,7 +489,7 @@ __global__ void k_fixup_compute(StepArgs a, const double* __restrict__ pv)
   }
   if (a.rec_fixset) a.rec_fixset[z] = (unsigned char)set;
   int rc = limit_gamma(gamma, pr, g);
-  if (rc) report_fail(a.sc, rc, i, j);
+  if (rc) report_fail(a.sc, a.phase0 + PH_FIXUP, rc, zone_order(i, j));
 #pragma unroll
   for (int k = 0; k <= U3; k++) a.fixbuf[k * pl + z] = pr[k];
 }

@@ -63,7 +63,7 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   if (!rc) rc = vchar_of(p_l, ql, dir, g, gam, cmax_l, cmin_l);
   if (!rc) rc = vchar_of(p_r, qr, dir, g, gam, cmax_r, cmin_r);
   if (rc) {
-    report_fail(a.sc, rc, i, j);
+    report_fail(a.sc, a.phase0 + (dir == 1 ? PH_FACE1 : PH_FACE2), rc, zone_order(i, j));
     cmax_l = cmin_l = cmax_r = cmin_r = T(0.);
   }
   // cminmax_calc, step_ch.c:1095-1148
@@ -239,7 +239,7 @@ __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>
   if (frho > pfz[RHO]) pfz[RHO] = frho;
   if (fu > pfz[UU]) pfz[UU] = fu;
   int rc = limit_gamma(a.pp.gammamax, pfz, g);
-  if (rc) report_fail(a.sc, rc, i, j);
+  if (rc) report_fail(a.sc, a.phase0 + PH_UPDATE, rc, zone_order(i, j));
 #pragma unroll
   for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
 }
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
     // GRMHD-only, fixup.c:293); pflag is left as it was
     int rc = utoprim_ffde(U, g, pfz, a.pp.gammamax);
     if (!rc) rc = limit_gamma(a.pp.gammamax, pfz, g);
-    if (rc) report_fail(a.sc, rc, i, j);
+    if (rc) report_fail(a.sc, a.phase0 + PH_UPDATE, rc, zone_order(i, j));
 #pragma unroll
     for (int k = 0; k < NPR; k++) pf[k * pl + z] = pfz[k];
     return;

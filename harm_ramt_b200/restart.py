@@ -60,22 +60,44 @@ def _header_line(h, accounting, rescaletype, lumvsr):
 
 def read_rdump(path):
     """Returns dict(header=dict, accounting=list, rescaletype=int,
-    lumvsr=list, prims=[n1, n2, 8] active zones)."""
+    lumvsr=list, prims=[n1, n2, 8] active zones).  A file cut short or
+    holding a token that is not a number raises ValueError naming the file
+    and the part that is missing or bad; no partial state is returned."""
     with open(path, "r") as f:
         first = f.readline()
         rest = f.read()
     tok = first.split()
     nfixed = len(HEADER_FIELDS)
+    if len(tok) < nfixed:
+        raise ValueError(f"rdump {path}: header holds {len(tok)} of its {nfixed} fixed fields (file cut short?)")
     h = {}
     for (name, conv), s in zip(HEADER_FIELDS, tok[:nfixed]):
-        h[name] = float(s) if conv == "g" else int(s)
+        try:
+            h[name] = float(s) if conv == "g" else int(s)
+        except ValueError:
+            raise ValueError(f"rdump {path}: header field {name} = {s!r} is not a number") from None
     n1, n2 = h["totalsize1"], h["totalsize2"]
-    acc = [float(x) for x in tok[nfixed:nfixed + ACCOUNTING_DOUBLES]]
-    resc = int(tok[nfixed + ACCOUNTING_DOUBLES])
-    lum = [float(x) for x in tok[nfixed + ACCOUNTING_DOUBLES + 1:]]
-    vals = np.array(rest.split(), dtype=np.float64)
+    if n1 <= 0 or n2 <= 0:
+        raise ValueError(f"rdump {path}: grid {n1} x {n2} in the header")
+    ntail = ACCOUNTING_DOUBLES + 1 + n1
+    if len(tok) != nfixed + ntail:
+        raise ValueError(f"rdump {path}: header holds {len(tok) - nfixed} accounting values where the "
+                         f"{n1}-zone grid needs {ntail} (file cut short?)")
+    try:
+        acc = [float(x) for x in tok[nfixed:nfixed + ACCOUNTING_DOUBLES]]
+        resc = int(tok[nfixed + ACCOUNTING_DOUBLES])
+        lum = [float(x) for x in tok[nfixed + ACCOUNTING_DOUBLES + 1:]]
+    except ValueError as e:
+        raise ValueError(f"rdump {path}: bad accounting value in the header ({e})") from None
+    try:
+        vals = np.array(rest.split(), dtype=np.float64)
+    except ValueError as e:
+        raise ValueError(f"rdump {path}: a primitive is not a number ({e})") from None
     if vals.size != n1 * n2 * NPR:
-        raise ValueError(f"{path}: {vals.size} values for a {n1} x {n2} grid")
+        raise ValueError(f"rdump {path}: {vals.size} values for a {n1} x {n2} grid of {NPR} primitives "
+                         f"(file cut short?)")
+    if not np.isfinite(vals).all():
+        raise ValueError(f"rdump {path}: {int((~np.isfinite(vals)).sum())} primitives are not finite")
     # DUMPLOOP order: j outer, i inner (global.h:1047)
     prims = vals.reshape(n2, n1, NPR).transpose(1, 0, 2).copy()
     return dict(header=h, accounting=acc, rescaletype=resc, lumvsr=lum, prims=prims)

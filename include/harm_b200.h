@@ -7,7 +7,7 @@
  * which reads and writes the reference's globals p, pk, pflag, dt, t,
  * realnstep and the geometry tables gcov/gcon/gdet/conn (defs.h:4-309).
  * A host shim that replaces step_ch() calls harm_step() on a context that
- * holds device-resident copies of those arrays (see INTEGRATION.md).
+ * holds device-resident copies of those arrays.
  *
  * Array arguments use the reference's own memory layout (defs.h) over the
  * full grid including NG = 3 ghost zones per side, n1m = n1 + 6 rows of
@@ -102,7 +102,14 @@ typedef struct harm_config {
 
 typedef struct harm_status {
   int fail_code;                 /* reference fail() code, 0 if none */
-  int fail_i, fail_j;            /* zone of the first fatal check */
+  int fail_i, fail_j;            /* zone of the first fatal check: of the kernels
+                                    that reported one, the first in the reference's
+                                    order of the step (x1 faces, x2 faces, update,
+                                    bound, repairs, bound; per substep), the first
+                                    zone of that pass in its loop order (i outer,
+                                    j inner) -- the zone and code the reference's
+                                    fail() reports (fail.c:4-57) for that state,
+                                    independent of thread scheduling */
   int fixups;                    /* zones repaired by fixup_utoprim since harm_set_time */
   long long realnstep;
   double t, dt;                  /* time and the next step's dt */
@@ -110,6 +117,11 @@ typedef struct harm_status {
   int chk_multi;                 /* substeps since harm_set_time whose check-solution
                                     sweep (fixup.c:388-488) needed more than one
                                     parallel round */
+  int deferred;                  /* inversions since harm_set_time that needed more
+                                    than 16 Newton iterations (redone by the tail
+                                    kernel with the reference's limit of 200) */
+  long long fail_step;           /* realnstep at the start of the step whose fatal
+                                    check is reported (-1 if none) */
 } harm_status;
 
 typedef struct harm_ctx harm_ctx;

@@ -36,10 +36,11 @@ Build patches (each one asserted to apply exactly):
      hash of the iterate (same function as the GPU kernel and the C
      restatement use), so that the factor no longer depends on a serial
      global RNG stream.
- 12. init.fishmon.c init_grid()/init_global() and dump.c dump() are renamed;
-     ref_harness.c wraps the first two to apply the benchmark knobs
-     (defcoord 0, Rin = 0.98 r_h, MC/PARA, HLL/LAXF, RK2, courant, floors)
-     and turns dump files off.
+ 12. init.fishmon.c init_grid()/init_global(), dump.c dump() and fail.c
+     fail() are renamed; ref_harness.c wraps the first two to apply the
+     benchmark knobs (defcoord 0, Rin = 0.98 r_h, MC/PARA, HLL/LAXF, RK2,
+     courant, floors), turns dump files off, and records the code and zone
+     of the first fail() call before calling the original.
  13. compiled -O2 -ffp-contract=off -fno-fast-math so that no FMA
      contraction changes the FP64 rounding.
 
@@ -137,6 +138,7 @@ def patch_tree(bdir, problem, n1, n2):
         return t
     edit("init.c", ini)
     edit("dump.c", lambda t, f: sub1(t, "int dump(long dump_cnt)\n", "int hr_orig_dump(long dump_cnt)\n", f))
+    edit("fail.c", lambda t, f: sub1(t, "int fail(int fail_type)\n", "int hr_orig_fail(int fail_type)\n", f))
 
     def logfix(t, f):
         # every vfprintf(X, format, arglist) consumes a private copy of the list
@@ -219,7 +221,8 @@ def build(src, problem, n1, n2, jobs, force=False):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=os.environ.get("HARM_REFERENCE_SRC", "/root/reference"),
+                    help="the reference source tree (default: $HARM_REFERENCE_SRC)")
     ap.add_argument("--problem", default="torus", choices=sorted(PROBLEMS))
     ap.add_argument("--sizes", default="16x16,32x32,64x64,128x128")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)

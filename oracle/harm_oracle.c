@@ -93,7 +93,8 @@ struct ho_state {
   long ccalls;        /* current_calc_1's static call count */
   double clastdt;     /* and its static lastdt */
   long ncb;
-  int fail;
+  int fail, fail_i, fail_j; /* first fatal check of the last ho_step: code and zone (fail.c:4-57 reports
+                               the zone of the last get_geometry call, i.e. the zone or face being worked on) */
   /* inputs of the inversions that failed (test fixtures for the retry
      chain): zone, U in the evolved form, the guess; up to rec_max */
   int rec_max, rec_n;
@@ -105,6 +106,16 @@ struct ho_state {
 static inline long zid(const ho_state *s, int i, int j) { return (long)(i + NG) * s->n2m + (j + NG); }
 #define P(arr, i, j) ((arr) + zid(s, (i), (j)) * NPR)
 #define FL(arr, i, j) ((arr) + zid(s, (i), (j)) * NFL)
+/* records the first fatal check (code rc at zone or face i, j) and passes rc on */
+static int failat(ho_state *s, int rc, int i, int j)
+{
+  if (rc && !s->fail) {
+    s->fail = rc;
+    s->fail_i = i;
+    s->fail_j = j;
+  }
+  return rc;
+}
 
 typedef struct {
   const double *gcov; /* 16, row-major */
@@ -430,8 +441,8 @@ static int fluxcalc(ho_state *s, const double *pb, double *F, int dir, double *n
       geo g = getgeo(s, i, j, face);
       if (dir == 1) p_l[B1] = p_r[B1] = 0.5 * (p_l[B1] + p_r[B1]);
       else p_l[B2] = p_r[B2] = 0.5 * (p_l[B2] + p_r[B2]);
-      if ((rc = limit_gamma(s->c.gammamax, p_l, &g))) return rc;
-      if ((rc = limit_gamma(s->c.gammamax, p_r, &g))) return rc;
+      if ((rc = limit_gamma(s->c.gammamax, p_l, &g))) return failat(s, rc, i, j);
+      if ((rc = limit_gamma(s->c.gammamax, p_r, &g))) return failat(s, rc, i, j);
       ostate ql, qr;
       state_of(p_l, &g, &ql);
       state_of(p_r, &g, &qr);
@@ -440,8 +451,8 @@ static int fluxcalc(ho_state *s, const double *pb, double *F, int dir, double *n
       flux_of(p_l, &ql, 0, &g, s->c.gam, ffde, U_l);
       flux_of(p_r, &qr, 0, &g, s->c.gam, ffde, U_r);
       double cmax_l, cmin_l, cmax_r, cmin_r;
-      if ((rc = vchar_of(p_l, &ql, dir, &g, s->c.gam, ffde, &cmax_l, &cmin_l))) return rc;
-      if ((rc = vchar_of(p_r, &qr, dir, &g, s->c.gam, ffde, &cmax_r, &cmin_r))) return rc;
+      if ((rc = vchar_of(p_l, &ql, dir, &g, s->c.gam, ffde, &cmax_l, &cmin_l))) return failat(s, rc, i, j);
+      if ((rc = vchar_of(p_r, &qr, dir, &g, s->c.gam, ffde, &cmax_r, &cmin_r))) return failat(s, rc, i, j);
       double lmin = rmin(cmin_l, cmin_r);
       double lmax = rmax(cmax_l, cmax_r);
       lmin = fabs(rmax(0., -lmin));
@@ -811,8 +822,8 @@ static int bound_prims_star(ho_state *s, double *pv)
     }
     for (i = -1; i >= -NG; i--) {
       geo g = getgeo(s, i, j, CENT);
-      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
-      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return failat(s, rc, i, j);
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return failat(s, rc, i, j);
     }
   }
   for (j = 0; j < n2; j++) {
@@ -826,8 +837,8 @@ static int bound_prims_star(ho_state *s, double *pv)
     }
     for (i = n1; i <= n1 - 1 + NG; i++) {
       geo g = getgeo(s, i, j, CENT);
-      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
-      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return failat(s, rc, i, j);
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return failat(s, rc, i, j);
     }
   }
 #undef GD
@@ -852,8 +863,8 @@ static int bound_prims(ho_state *s, double *pv)
       for (k = 0; k < NPR; k++) P(pv, i, j)[k] = P(pv, 0, j)[k];
     for (i = -1; i >= -NG; i--) {
       geo g = getgeo(s, i, j, CENT);
-      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
-      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return failat(s, rc, i, j);
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return failat(s, rc, i, j);
     }
   }
   for (j = 0; j < n2; j++) {
@@ -861,8 +872,8 @@ static int bound_prims(ho_state *s, double *pv)
       for (k = 0; k < NPR; k++) P(pv, i, j)[k] = P(pv, n1 - 1, j)[k];
     for (i = n1; i <= n1 - 1 + NG; i++) {
       geo g = getgeo(s, i, j, CENT);
-      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return rc;
-      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return rc;
+      if ((rc = inflow_check_x1(s, P(pv, i, j), &g))) return failat(s, rc, i, j);
+      if ((rc = limit_gamma(s->c.gammamax, P(pv, i, j), &g))) return failat(s, rc, i, j);
     }
   }
   for (i = -NG; i <= n1 - 1 + NG; i++)
@@ -1016,7 +1027,7 @@ static int fixup_utoprim(ho_state *s, double *pv, int *pf)
             pr[k] = 0.5 * (0.25 * (PA(i, j + 1)[k] + PA(i, j - 1)[k] + PA(i - 1, j)[k] + PA(i + 1, j)[k]) +
                            0.25 * (PA(i + 1, j + 1)[k] + PA(i + 1, j - 1)[k] + PA(i - 1, j + 1)[k] + PA(i - 1, j - 1)[k]));
       }
-      if ((rc = limit_gamma(gamma, pr, &g))) return rc;
+      if ((rc = limit_gamma(gamma, pr, &g))) return failat(s, rc, i, j);
       FL(pf, i, j)[F_FAIL] = PF_FIXED;
     }
 #undef GOOD
@@ -1058,7 +1069,7 @@ static int advance(ho_state *s, const double *pi, const double *pb, double *pf, 
       for (k = 0; k < NPR; k++) ul[k] = Uf[k] = CUf[0] * Ui[k] + CUf[1] * ul[k] + CUf[2] * dt * (dUr[k] + dUg[k]);
       for (k = 0; k < NPR; k++) un[k] += Cunew[0] * Ui[k] + Cunew[1] * dt * (dUr[k] + dUg[k]) + Cunew[2] * Uf[k];
       if (s->c.eom) {
-        if ((rc = utoprim_ffde(s, last ? un : Uf, &g, pfz))) return rc;
+        if ((rc = utoprim_ffde(s, last ? un : Uf, &g, pfz))) return failat(s, rc, i, j);
       } else {
         double guess[NPR];
         for (k = 0; k < NPR; k++) guess[k] = pfz[k];
@@ -1078,7 +1089,7 @@ static int advance(ho_state *s, const double *pi, const double *pb, double *pf, 
         if (fl[0] > pfz[RHO]) pfz[RHO] = fl[0];
         if (fl[1] > pfz[UU]) pfz[UU] = fl[1];
       }
-      if ((rc = limit_gamma(s->c.gammamax, pfz, &g))) return rc;
+      if ((rc = limit_gamma(s->c.gammamax, pfz, &g))) return failat(s, rc, i, j);
       for (k = 0; k < NPR; k++) P(pf, i, j)[k] = pfz[k];
     }
   *ndt = s->c.defcon * 1. / (1. / ndt1 + 1. / ndt2);
@@ -1326,6 +1337,7 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
   double ndt = 0.0;
   int to, rc, moved;
   s->pcur = p;
+  s->fail = s->fail_i = s->fail_j = 0;
   for (to = 0; to < 2; to++) {
     const double *pi = p;
     const double *pb = (to == 0) ? p : s->pk0;
@@ -1350,4 +1362,11 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
   if (moved) s->dt_free = ndt; /* a step at dt = 0 (past the end time) keeps the last one */
   if (*t + *dt > s->c.tf) *dt = s->c.tf - *t;
   return 0;
+}
+
+void ho_get_fail(const ho_state *s, int *out)
+{
+  out[0] = s->fail;
+  out[1] = s->fail_i;
+  out[2] = s->fail_j;
 }

@@ -81,6 +81,11 @@ int ho_record_failures(ho_state *s, int max);
    failure; arrays sized for the max given); returns their number */
 int ho_get_failures(const ho_state *s, int *ij, double *U, double *pr);
 
+/* the first fatal check of the last ho_step: out[0] = FAIL_* code (0 if
+   none), out[1..2] = the zone or face (i, j) being worked on, as the
+   reference's fail() reports it (fail.c:4-57) */
+void ho_get_fail(const ho_state *s, int *out);
+
 /* the deterministic cycle-break factor (shared with the GPU kernel) */
 double ho_cycle_break_uniform(double x0, double x1, int n_iter);
 

@@ -104,6 +104,23 @@ int init_global(void)
   return 0;
 }
 
+/* patch 12: the first fatal check of a step, as fail() (fail.c:4-57)
+   reports it: the code and the zone of the last get_geometry() call
+   (icurr, jcurr, set with JONCHECKS 1, phys.c:757) */
+extern int hr_orig_fail(int fail_type);
+static int hr_fail_code = 0, hr_fail_i = 0, hr_fail_j = 0;
+int fail(int fail_type)
+{
+  if (whocalleducon != 1 && hr_fail_code == 0) {
+    hr_fail_code = fail_type;
+    hr_fail_i = icurr;
+    hr_fail_j = jcurr;
+  }
+  return hr_orig_fail(fail_type);
+}
+void hr_get_fail(int *out) { out[0] = hr_fail_code; out[1] = hr_fail_i; out[2] = hr_fail_j; }
+void hr_clear_fail(void) { hr_fail_code = hr_fail_i = hr_fail_j = 0; failed = 0; }
+
 /* patch 12: no dump files from the oracle */
 int dump(long dump_cnt) { (void)dump_cnt; return 0; }
 

@@ -71,6 +71,8 @@ def oracle_lib():
         lib.ho_cycle_break_uniform.restype = ctypes.c_double
         lib.ho_record_failures.argtypes = [vp, ctypes.c_int]
         lib.ho_get_failures.argtypes = [vp, ctypes.POINTER(ctypes.c_int), dp, dp]
+        lib.ho_get_fail.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        lib.ho_get_fail.restype = None
         _oracle = lib
     return _oracle
 
@@ -132,6 +134,12 @@ class Oracle:
         f2 = np.zeros((self.n1m, self.n2m, 8))
         self.lib.ho_get_fluxes(self.h, _dp(f1), _dp(f2))
         return f1, f2
+
+    def fail(self):
+        """(code, i, j) of the first fatal check of the last step (code 0: none)"""
+        out = np.zeros(3, dtype=np.int32)
+        self.lib.ho_get_fail(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return tuple(int(v) for v in out)
 
     def ncyclebreak(self):
         return self.lib.ho_ncyclebreak(self.h)
@@ -330,6 +338,63 @@ def ref_utoprim_pick(n1, n2, methods, ij, U, pr, problem="torusta", timeout=1800
     code = ("import sys, numpy as np; sys.path.insert(0, %r); import harmtest; d = np.load(%r); "
             "harmtest._ref_pick_worker(%r, %r, d['ij'], d['U'], d['pr'], %r)"
             % (os.path.dirname(os.path.abspath(__file__)), inp, path, list(methods), out))
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed (rc=%d): %s" % (r.returncode, r.stderr[-2000:]))
+        with open(out, "rb") as f:
+            return pickle.load(f)
+    finally:
+        os.unlink(out)
+        os.unlink(inp)
+
+
+def _ref_fail_worker(libpath, lim, flux, prims, outpath):
+    """Runs in a child process: reference init, then its step from the given
+    state; records the step's return and the first fail() (code, i, j)."""
+    import pickle
+    lib = ctypes.CDLL(libpath)
+    lib.hr_configure.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 ctypes.c_double]
+    lib.hr_configure(lim, flux, 2, 0.8, 0, 1e30)
+    work = tempfile.mkdtemp(prefix="harmref_")
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved, saved1 = os.dup(2), os.dup(1)
+    os.dup2(devnull, 2)
+    os.dup2(devnull, 1)
+    try:
+        if lib.hr_init(work.encode()) != 0:
+            raise RuntimeError("reference init failed")
+        V = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        lib.hr_set_prims(V(np.ascontiguousarray(prims, dtype=np.float64)))
+        lib.hr_clear_fail()
+        rc = lib.hr_step(1)
+        out = np.zeros(3, dtype=np.int32)
+        lib.hr_get_fail(V(out))
+    finally:
+        os.dup2(saved, 2)
+        os.dup2(saved1, 1)
+    with open(outpath, "wb") as f:
+        pickle.dump(dict(rc=rc, fail=tuple(int(v) for v in out)), f, protocol=4)
+
+
+def ref_fail(n1, n2, prims, lim=3, flux=1, problem="torus", timeout=600):
+    """The compiled reference's step from `prims` (reference layout, ghosts
+    included): {rc, fail: (code, i, j)} of its first fail() call, or None
+    when that build is absent."""
+    import pickle
+    import sys
+    path = ref_lib_path(n1, n2, problem)
+    if path is None:
+        return None
+    fd, out = tempfile.mkstemp(suffix=".pkl", prefix="harmref_")
+    os.close(fd)
+    fi, inp = tempfile.mkstemp(suffix=".npy", prefix="harmref_")
+    os.close(fi)
+    np.save(inp, np.ascontiguousarray(prims, dtype=np.float64))
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import harmtest; "
+            "harmtest._ref_fail_worker(%r, %d, %d, np.load(%r), %r)"
+            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, inp, out))
     try:
         r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
