@@ -47,6 +47,12 @@ def parse():
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--lim", default="para", choices=["para", "mc"])
     ap.add_argument("--flux", default="hll", choices=["hll", "laxf"])
+    ap.add_argument("--fluxadjust", type=int, default=3, choices=[0, 1, 2, 3],
+                    help="FLUXADJUST: 0 every face uses --flux; 1-3 the per-zone HLL/LAXF switch of the 512^2 and "
+                         "1024^2 configuration (FLUXBSQORHOANDU is 3)")
+    ap.add_argument("--window-steps", type=int, default=20,
+                    help="steps of the same-window comparison: steps 3.. from init, the window the reference arm "
+                         "times, with the diagnostic currents on as the reference's step_ch() computes them")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--evolve", type=int, default=400,
                     help="untimed steps from init before warm-up, so that the timed steps see a developed flow")
@@ -70,6 +76,15 @@ def parse():
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="reference arm: seconds of stepping per process after which it stops early")
     return ap.parse_args()
+
+
+def workload(a, n):
+    """The workload description shared by both arms."""
+    sw = {0: "fixed " + a.flux.upper(), 1: "HLL/LAXF switch (FLUXBSQORHO)", 2: "HLL/LAXF switch (FLUXBSQOU)",
+          3: "HLL/LAXF switch (FLUXBSQORHOANDU)"}[a.fluxadjust]
+    return {"workload": f"{n}x{n} Fishbone-Moncrief torus, MKS a=0.9375, FP64, {a.lim.upper()} reconstruction, "
+                        f"{a.flux.upper()} flux with per-zone {sw}, flux-CT, 2D Newton con-to-prim, RK2 midpoint, "
+                        "courant 0.8", "n1": n, "n2": n, "fluxadjust": a.fluxadjust}
 
 
 def peaks():
@@ -127,9 +142,22 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference
-def _ref_lib(n):
-    p = os.path.join(ROOT, "oracle", "_ref", f"libharmref_torus_{n}x{n}.so")
-    return p if os.path.exists(p) else None
+def _ref_lib(n, fluxadjust):
+    """The reference's CPU step for the workload: its sources as the parity
+    build patched them (FLUXADJUST FLUXBSQORHOANDU for the switch), compiled
+    -O3 -march=native -ffp-contract=off for this host (oracle/build_ref.py
+    --native, from the scratch tree the parity build left in oracle/_ref);
+    the parity build itself (-O2) if that fails.  (path, flags) or None."""
+    problem = "torusfa" if fluxadjust else "torus"
+    parity = os.path.join(ROOT, "oracle", "_ref", f"libharmref_{problem}_{n}x{n}.so")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "build_ref.py"), "--native", "--problem", problem,
+                        "--sizes", f"{n}x{n}"], capture_output=True, text=True)
+    lines = r.stdout.strip().splitlines()
+    if r.returncode == 0 and lines and os.path.exists(lines[-1]):
+        return lines[-1], "-O3 -march=native -ffp-contract=off"
+    if os.path.exists(parity):
+        return parity, "-O2 -ffp-contract=off (native build failed: %s)" % (r.stderr.strip().splitlines() or ["?"])[-1]
+    return None
 
 
 REF_WORKER = r"""
@@ -151,13 +179,10 @@ os.write(sv, (" ".join("%.6f" % t for t in ts) + "\n").encode())
 """
 
 
-def run_reference_procs(n, lim, flux, nsteps, nprocs, budget_s=1e9):
-    """nprocs independent reference processes (one torus each); per-step wall
-    times of each (a process stops early once budget_s of stepping is spent).
-    Returns a list of lists."""
-    lib = _ref_lib(n)
-    if lib is None:
-        return None
+def run_reference_procs(lib, lim, flux, nsteps, nprocs, budget_s=1e9):
+    """nprocs independent reference processes (one torus each, library
+    `lib`); per-step wall times of each (a process stops early once budget_s
+    of stepping is spent).  Returns a list of lists."""
     procs = [subprocess.Popen([sys.executable, "-c", REF_WORKER, lib, str(lim), str(nsteps), str(flux), str(budget_s)],
                               stdout=subprocess.PIPE, stderr=subprocess.DEVNULL) for _ in range(nprocs)]
     out = []
@@ -175,6 +200,11 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
+# the step window both arms time for the same-window comparison: steps
+# WINDOW_FIRST.. from init (the reference's step_ch() from its own init())
+WINDOW_FIRST = 3
+
+
 def reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -182,20 +212,22 @@ def reference_arm(a):
     n = a.n
     lim = 4 if a.lim == "para" else 3
     flux = 1 if a.flux == "hll" else 0
-    cfg = {"workload": f"{n}x{n} Fishbone-Moncrief torus, MKS a=0.9375, FP64, {a.lim.upper()} + {a.flux.upper()}, "
-                       "flux-CT, 2D Newton con-to-prim, RK2 midpoint, courant 0.8", "n1": n, "n2": n,
-           "parallelism": "one process per host core, independent tori"}
-    if _ref_lib(n) is None:
-        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libharmref_torus_%dx%d.so "
+    cfg = workload(a, n)
+    cfg["parallelism"] = "one process per host core, independent tori"
+    lib = _ref_lib(n, a.fluxadjust)
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libharmref_*_%dx%d.so "
                                                               "not present (built from the reference sources by "
                                                               "__graft_entry__.build())" % (n, n)}))
         return 0
+    lib, cflags = lib
     nprocs = max(1, min(cpu_cores(), 16))
     t0 = time.time()
-    # a reference step of this torus takes seconds per core: warm-up and the
-    # timed steps are bounded by a wall budget so the run ends in minutes
-    warm = min(a.warmup, 2)
-    per = run_reference_procs(n, lim, flux, warm + a.steps, nprocs, budget_s=a.ref_budget)
+    # a reference step of this torus takes seconds per core: the timed steps
+    # are the same-window steps (WINDOW_FIRST.. from init), bounded by a wall
+    # budget so the run ends in minutes
+    warm = WINDOW_FIRST - 1
+    per = run_reference_procs(lib, lim, flux, warm + min(a.steps, a.window_steps), nprocs, budget_s=a.ref_budget)
     per = [p for p in per if len(p) > warm]
     if not per:
         print(json.dumps({"impl": "reference", "unavailable": "reference step failed"}))
@@ -206,17 +238,33 @@ def reference_arm(a):
     step_times = [max(p[warm + k] for p in per) for k in range(ktimed)]
     tstep = sum(step_times) / len(step_times)
     value = len(per) * n * n / tstep
+    window = f"steps {WINDOW_FIRST}-{WINDOW_FIRST + ktimed - 1} from init"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": ktimed, "warmup": warm,
             "steps_requested": a.steps, "warmup_requested": a.warmup,
             "ms_per_step": tstep * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded torus of the reference's own init)", "config": cfg,
-            "impl": "reference",
+            "impl": "reference", "window": window,
+            "work": "the reference's step_ch(), which computes the diagnostic currents every step "
+                    "(WHICHCURRENTCALC 1, step_ch.c:143-156)",
+            "build": cflags, "host_cpu": _host_cpu(),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(per), "kind": "reference",
                              "sample": f"{len(per)} processes x ({warm} warm-up + {ktimed} timed) reference "
-                                       f"steps of a {n}x{n} torus after init; wall {time.time() - t0:.0f}s"},
+                                       f"steps of a {n}x{n} torus ({window}), built {cflags}; wall "
+                                       f"{time.time() - t0:.0f}s"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def _host_cpu():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # ------------------------------------------------------------------ b200 arm
@@ -252,7 +300,8 @@ def b200_arm(a):
     n = a.n
     lim = hb.LIM_PARA if a.lim == "para" else hb.LIM_MC
     flux = hb.FLUX_HLL if a.flux == "hll" else hb.FLUX_LAXF
-    h, geom, p0 = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream)
+    fa = a.fluxadjust
+    h, geom, p0 = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, fluxadjust=fa)
 
     def barrier():
         if dist is not None:
@@ -340,31 +389,32 @@ def b200_arm(a):
     sizes = None
     if a.sizes:
         sizes = sizes_leg(a, hb, stream, lim, barrier, dist)
+    window = same_window_leg(a, hb, stream, lim, flux, barrier, dist) if a.window_steps > 0 else None
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        per = run_reference_procs(n, 4 if a.lim == "para" else 3, 1 if a.flux == "hll" else 0, 2, 1)
-        if per and len(per[0]) == 2:
-            t1 = per[0][1]
+        rl = _ref_lib(n, a.fluxadjust)
+        per = run_reference_procs(rl[0], 4 if a.lim == "para" else 3, 1 if a.flux == "hll" else 0, WINDOW_FIRST, 1) \
+            if rl else None
+        if per and len(per[0]) == WINDOW_FIRST:
+            t1 = per[0][-1]
             cpu = {"value": n * n / t1, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": f"reference step_ch() of the {n}x{n} torus on one host core, second step after init "
-                             f"({t1:.2f} s)"}
+                   "sample": f"reference step_ch() of the {n}x{n} torus on one host core, step {WINDOW_FIRST} from "
+                             f"init ({t1:.2f} s), built {rl[1]}"}
     h.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Fishbone-Moncrief torus, init of "
                                                              "init.fishmon.c restated on the host)",
-                "config": {"workload": f"{n}x{n} Fishbone-Moncrief torus, MKS a=0.9375, FP64, "
-                                       f"{a.lim.upper()} + {a.flux.upper()}, flux-CT, 2D Newton con-to-prim, "
-                                       "RK2 midpoint, courant 0.8", "n1": n, "n2": n,
+                "config": {**workload(a, n),
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "l2": "working set per step (geometry 126 planes x %.1f MB) exceeds L2" %
                                  ((n + 6) * (n + 6) * 8 / 1e6),
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
-                "ensemble": ens, "adjoint": adj, "rows": rows, "sizes": sizes,
+                "ensemble": ens, "adjoint": adj, "rows": rows, "sizes": sizes, "same_window": window,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
@@ -374,32 +424,83 @@ def b200_arm(a):
 
 
 def sizes_leg(a, hb, stream, lim, barrier, dist):
-    """The same torus at the other grid sizes and with the other Riemann
-    solver (HLL and LAXF at each size in --sizes): whole-job zone-cycles/s
-    after 100 untimed steps, device time of 100 steps (max over ranks)."""
+    """The configuration at the other grid sizes of --sizes (the per-zone
+    switch as in the headline), and at the headline size each fixed Riemann
+    solver (fluxadjust 0, HLL and LAXF): whole-job zone-cycles/s after 100
+    untimed steps, device time of 100 steps (max over ranks)."""
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    flux = hb.FLUX_HLL if a.flux == "hll" else hb.FLUX_LAXF
+    runs = [(n, flux, a.fluxadjust, f"{a.flux}_switch{a.fluxadjust}") for n in [int(x) for x in a.sizes.split(",") if x]
+            if n != a.n]
+    runs += [(a.n, hb.FLUX_HLL, 0, "hll_fixed"), (a.n, hb.FLUX_LAXF, 0, "laxf_fixed")]
     out = {}
-    for n in [int(s) for s in a.sizes.split(",") if s]:
-        for fname, fl in (("hll", hb.FLUX_HLL), ("laxf", hb.FLUX_LAXF)):
-            if n == a.n and fl == (hb.FLUX_HLL if a.flux == "hll" else hb.FLUX_LAXF):
-                continue  # the headline line itself
-            h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=fl, stream=stream.cuda_stream)
-            h.step_ch(100)
-            h.sync()
-            barrier()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            h.step_ch(100)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / 100
-            h.sync()
-            h.close()
-            out[f"{n}_{fname}"] = {"value": aggregate_rate(world, n * n, ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-                                   "workload": f"{n}x{n} torus, FP64, {a.lim.upper()} + {fname.upper()}, "
-                                               "steps 101-200 from init"}
+    for n, fl, fa, name in runs:
+        h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=fl, stream=stream.cuda_stream, fluxadjust=fa)
+        h.step_ch(100)
+        h.sync()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.step_ch(100)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / 100
+        h.sync()
+        h.close()
+        out[f"{n}_{name}"] = {"value": aggregate_rate(world, n * n, ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                              "workload": f"{n}x{n} torus, FP64, {a.lim.upper()} + "
+                                          f"{['LAXF', 'HLL'][fl]}, fluxadjust {fa}, steps 101-200 from init"}
+    return out
+
+
+def same_window_leg(a, hb, stream, lim, flux, barrier, dist):
+    """The reference arm's window and work on the device: a fresh torus from
+    init, steps WINDOW_FIRST.. (a.window_steps of them), the diagnostic
+    currents on as in the reference's step_ch().  (1) device-resident state,
+    CUDA events; (2) end to end through the C ABI from host buffers: each
+    step uploads the state, steps and reads state and flags back."""
+    import torch
+    n = a.n
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    K = a.window_steps
+    out = {"window": f"steps {WINDOW_FIRST}-{WINDOW_FIRST + K - 1} from init",
+           "work": "step_ch() with the diagnostic currents (J^mu, Faraday slots) every step"}
+    h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, currents=True,
+                               fluxadjust=a.fluxadjust)
+    h.step_ch(WINDOW_FIRST - 1)
+    h.sync()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h.step_ch(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / K
+    h.close()
+    out["value"] = aggregate_rate(world, n * n, ms * 1e-3)
+    out["unit"] = UNIT
+    out["ms_per_step"] = ms
+    h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, currents=True,
+                               fluxadjust=a.fluxadjust)
+    h.step_ch(WINDOW_FIRST - 1)
+    bufs = [(hb.pinned_empty((n + 6, n + 6, 8)), hb.pinned_empty((n + 6, n + 6, 5), np.int32)) for _ in range(2)]
+    h.get_prims(out=bufs[0])
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(K):
+        src, dst = bufs[k % 2], bufs[(k + 1) % 2]
+        h.set_prims(src[0], reset_gammacheck=False)
+        h.step_ch(1)
+        h.get_prims(out=dst)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / K, dist, "cuda")
+    h.close()
+    out["e2e"] = {"value": aggregate_rate(world, n * n, e2e_s), "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+                  "h2d_bytes_per_step": bufs[0][0].nbytes, "d2h_bytes_per_step": bufs[0][0].nbytes + bufs[0][1].nbytes}
     return out
 
 
@@ -428,7 +529,8 @@ def rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist):
 
     out = {}
     # (1) currents, developed flow
-    h, geom, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, currents=True)
+    h, geom, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, currents=True,
+                                  fluxadjust=a.fluxadjust)
     h.step_ch(a.evolve + a.warmup)
     h.sync()
     k = max(20, min(a.steps, 200))
@@ -456,7 +558,8 @@ def rows_leg(a, hb, stream, lim, flux, ms_step, barrier, dist):
     ks = 40
     res = {}
     for name, ta in (("with_chain", True), ("without_chain", False)):
-        h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, tryagain=ta)
+        h, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, stream=stream.cuda_stream, tryagain=ta,
+                                   fluxadjust=a.fluxadjust)
         h.step_ch(1)  # the graph
         h.sync()
         res[name] = timed(h, ks)
@@ -552,7 +655,8 @@ def ensemble_leg(a, hb, stream, lim, flux, barrier, dist):
         return max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
 
     for name, prec in (("fp64", hb.PREC_FP64), ("mixed", hb.PREC_MIXED)):
-        members = ens.build(hb, specs, lim=lim, fluxmethod=flux, precision=prec, stream=stream.cuda_stream)
+        members = ens.build(hb, specs, lim=lim, fluxmethod=flux, precision=prec, stream=stream.cuda_stream,
+                            fluxadjust=a.fluxadjust)
         tiles = {}
         for (h, p0), s in zip(members, specs):
             up, sm, _ = autotune.tune(h, reps=2, key=(s["n1"], s["n2"], prec, lim, flux))
@@ -598,7 +702,7 @@ def accuracy_curve(a, hb, stream, lim, flux):
     runs = {}
     for name in ("fp64", "mixed", "fp64_perturbed"):
         prec = hb.PREC_MIXED if name == "mixed" else hb.PREC_FP64
-        h, _, p0 = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=prec, tf=times[0],
+        h, _, p0 = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=prec, tf=times[0], fluxadjust=a.fluxadjust,
                                     stream=stream.cuda_stream)
         if name == "fp64_perturbed":
             rng = np.random.default_rng(20240607)
@@ -635,7 +739,8 @@ def mixed_precision_leg(a, hb, stream, lim, flux, value_fp64, barrier, dist):
     L1 errors against FP64 for runs from init to t = accuracy_t."""
     import torch
     n = a.n
-    hm, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=hb.PREC_MIXED, stream=stream.cuda_stream)
+    hm, _, _ = hb.torus_context(n, n, lim=lim, fluxmethod=flux, precision=hb.PREC_MIXED, stream=stream.cuda_stream,
+                                fluxadjust=a.fluxadjust)
     if a.evolve:
         hm.step_ch(a.evolve)
     hm.step_ch(a.warmup)

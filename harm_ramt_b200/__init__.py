@@ -61,7 +61,8 @@ class _Config(ctypes.Structure):
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("gammamax", ctypes.c_double),
                 ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
                 ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
-                ("omegastar", ctypes.c_double), ("currents", ctypes.c_int), ("tryagain", ctypes.c_int)]
+                ("omegastar", ctypes.c_double), ("currents", ctypes.c_int), ("tryagain", ctypes.c_int),
+                ("fluxadjust", ctypes.c_int), ("gammadamp", ctypes.c_double)]
 
 
 class _DumpHeader(ctypes.Structure):
@@ -99,7 +100,8 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_kernel_name", "harm_get_horizon", "harm_set_end_time", "harm_get_currents", "harm_write_dump",
            "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
            "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt",
-           "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint", "harm_invert_zones"]
+           "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint", "harm_invert_zones",
+           "harm_measure_fp64_peak"]
 
 
 def load_library(path=None):
@@ -156,6 +158,7 @@ def load_library(path=None):
     lib.harm_ensemble_destroy.argtypes = [vp]
     lib.harm_ensemble_destroy.restype = None
     lib.harm_torus_dump_coords.argtypes = [ctypes.POINTER(_TorusParams), ctypes.POINTER(_DumpHeader), dp]
+    lib.harm_measure_fp64_peak.argtypes = [dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
     if path is None:
@@ -257,13 +260,14 @@ class HarmGPU:
     def __init__(self, n1, n2, dx1, dx2, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, gam=4.0 / 3.0, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1.0e30,
                  precision=PREC_FP64, stream=None, eom=EOM_GRMHD, bc=BC_TORUS, omegastar=0.0, currents=False,
-                 tryagain=False):
+                 tryagain=False, fluxadjust=0, gammadamp=5.0):
         self.lib = load_library()
         self.n1, self.n2 = n1, n2
         self.n1m, self.n2m = n1 + 2 * NG, n2 + 2 * NG
         self.safe = safe
         cfg = _Config(n1, n2, lim, fluxmethod, eom, precision, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                      bsqorholimit, bsqoulimit, tf, bc, omegastar, int(bool(currents)), int(bool(tryagain)))
+                      bsqorholimit, bsqoulimit, tf, bc, omegastar, int(bool(currents)), int(bool(tryagain)),
+                      int(fluxadjust), float(gammadamp))
         h = ctypes.c_void_p()
         _check(self.lib.harm_create(ctypes.byref(cfg), ctypes.c_void_p(stream or 0), ctypes.byref(h)), "harm_create")
         self._h = h
@@ -445,6 +449,13 @@ class HarmGPU:
         return f1, f2
 
 
+def measure_fp64_peak():
+    """The device's FP64 instruction rates: {dadd, dmul, dfma} per second."""
+    out = np.zeros(3)
+    _check(load_library().harm_measure_fp64_peak(_dp(out)), "harm_measure_fp64_peak")
+    return dict(zip(("dadd", "dmul", "dfma"), out.tolist()))
+
+
 def pinned_empty(shape, dtype=np.float64):
     """A page-locked host array (allocated through torch), for fast
     host<->device copies of the reference-layout state."""
@@ -504,7 +515,7 @@ def torus_dump_coords(params):
 
 
 def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, precision=PREC_FP64, tf=1.0e30,
-                  stream=None, currents=False, tryagain=False, **torus_kw):
+                  stream=None, currents=False, tryagain=False, fluxadjust=0, **torus_kw):
     """Builds the benchmark torus on the host and returns (HarmGPU, geometry,
     initial prims) with the state uploaded, bounded and t=0, dt=1e-5 set as
     init_defglobal() leaves them (initbase.c:158)."""
@@ -513,7 +524,7 @@ def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, 
     p0 = torus_init(par, geom)
     h = HarmGPU(n1, n2, geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, cour=cour, gam=par.gam,
                 gammamax=par.gammamax, precision=precision, tf=tf, stream=stream, currents=currents,
-                tryagain=tryagain)
+                tryagain=tryagain, fluxadjust=fluxadjust)
     h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
     h.set_prims(p0)
     h.bound_prims()

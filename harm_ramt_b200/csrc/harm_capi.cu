@@ -23,7 +23,6 @@
 
 namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
-__global__ void k_bsqflags_ring(StepArgs a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
 __global__ void k_gammacheck(StepArgs a, double* pv, int poledeath);
@@ -31,7 +30,7 @@ __global__ void k_checksol(StepArgs a, const double* pv, int round);
 __global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
 __global__ void k_fixup_compute(StepArgs a, const double* pv);
 __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd);
-__global__ void k_dt_finalize(StepArgs a);
+__global__ void k_bound_fix(StepArgs a, double* pv);
 __global__ void k_faraday(StepArgs a, const double* pv);
 __global__ void k_current(StepArgs a);
 __global__ void k_currents_commit(StepArgs a);
@@ -77,7 +76,7 @@ struct harm_ctx {
   int *d_pflag, *d_worklist;
   double* d_stage;   // reference-layout prims staging buffer
   int* d_stagef;     // reference-layout pflag staging buffer
-  unsigned char *d_bsqf, *d_chk;
+  unsigned char *d_bsqf, *d_chk, *d_fluxf;
   DevScalars* d_sc;
   int nblocks_flux;
   int flux_by;       // k_flux rows per block (flux_rows)
@@ -124,6 +123,9 @@ struct harm_ctx {
     a.cur = d_cur;
     a.pp.currents = cfg.currents;
     a.pp.tryagain = cfg.tryagain;
+    a.pp.fluxadjust = cfg.fluxadjust;
+    a.pp.gammadamp = cfg.gammadamp;
+    a.fluxf = d_fluxf;
     a.rec_pinv = nullptr;
     a.rec_fixset = nullptr;
     a.bsqf_fused = nullptr;
@@ -147,9 +149,11 @@ static dim3 grid2(int ni, int nj, dim3 b) { return dim3((ni + b.x - 1) / b.x, (n
 // kernel classes of one step, in launch order (for per-kernel timing)
 enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_CHECKSOL, KC_CHECKSERIAL, KC_FIXC,
        KC_FIXA, KC_DT, KC_HORIZON, KC_FARADAY, KC_CURRENT, KC_COUNT };
+// (KC_FIXA: k_fixup_apply on the adjoint's recording path, k_bound_fix --
+// repairs, second bound and POLEDEATH in one kernel -- on every other)
 static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", "k_update", "k_bound", "k_poledeath",
                                                "k_gammacheck", "k_checksol", "k_checksol_serial", "k_fixup_compute",
-                                               "k_fixup_apply", "k_dt_finalize", "k_horizon", "k_faraday",
+                                               "k_bound_fix", "k_step_end", "k_horizon", "k_faraday",
                                                "k_current"};
 
 struct Timer {
@@ -198,16 +202,16 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
   cudaStream_t s = c->stream;
   const size_t pbytes = (size_t)NPR * c->gr.plane * sizeof(double), fbytes = (size_t)c->gr.plane * sizeof(int);
   if (rec) cudaMemcpyAsync(rec->pn, c->d_p, pbytes, cudaMemcpyDeviceToDevice, s);
-  // b^2 flags of the step's p: FP64 GRMHD sets the active zones' inside the
-  // first substep's k_update (from the state it forms anyway), the ring here
-  const bool fuse_bsq = (c->cfg.precision == HARM_PREC_FP64) && (c->cfg.eom == HARM_EOM_GRMHD);
-  if (fuse_bsq) {
-    const int nring = 2 * (n1 + 2) + 2 * n2;
-    k_bsqflags_ring<<<(nring + 127) / 128, 128, 0, s>>>(a, c->d_p);
-  } else {
+  // b^2 flags of the step's p: FP64 GRMHD sets them inside the first
+  // substep, the active zones' in k_update (from the state it forms anyway)
+  // and the one-zone ring's in k_emf; otherwise k_bsqflags first.  (With the
+  // flux switch every flag of the DQZLOOP range is needed before the first
+  // substep's fluxes, so they all come from k_bsqflags.)
+  const bool fuse_bsq = (c->cfg.precision == HARM_PREC_FP64) && (c->cfg.eom == HARM_EOM_GRMHD) && !c->cfg.fluxadjust;
+  if (!fuse_bsq) {
     k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
+    T.mark(s, KC_BSQ);
   }
-  T.mark(s, KC_BSQ);
   for (int sub = 0; sub < 2; sub++) {
     if (rec) {
       a.rec_pinv = rec->pinv[sub];
@@ -224,7 +228,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
     launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2, c->flux_by), fb, s, a, pb);
     T.mark(s, KC_FLUX);
-    launch_emf(mixed, grid2(n1 + 1, n2 + 1, b), b, s, a);
+    launch_emf(mixed, grid2(n1 + 2, n2 + 2, b), b, s, a, c->d_p);
     T.mark(s, KC_EMF);
     launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE, ffde ? 1 : 2);  // k_update and k_update_tail
@@ -256,18 +260,19 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     T.mark(s, KC_CHECKSERIAL);
     k_fixup_compute<<<grid2(n1, n2, b), b, 0, s>>>(a, pf);
     T.mark(s, KC_FIXC);
+    if (!rec) {
+      // repairs applied, second bound, POLEDEATH: one kernel
+      k_bound_fix<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf);
+      T.mark(s, KC_FIXA);
+      continue;
+    }
+    // the adjoint's recording keeps the state between the repairs and the
+    // second bound, so it runs them as separate kernels
     k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, 1);
-    T.mark(s, KC_FIXA);
-    if (rec) {
-      cudaMemcpyAsync(rec->pre2[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
-      cudaMemcpyAsync(rec->flag[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
-    }
+    cudaMemcpyAsync(rec->pre2[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(rec->flag[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 0);
-    T.mark(s, KC_BOUND);
-    if (poledeath) {
-      k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
-      T.mark(s, KC_POLE);
-    }
+    if (poledeath) k_poledeath<<<dim3((n1 + 127) / 128, 2), 128, 0, s>>>(a, pf);
   }
   a = a0;
   if (rec) cudaMemcpyAsync(rec->ph, c->d_pk0, pbytes, cudaMemcpyDeviceToDevice, s);
@@ -279,9 +284,8 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     k_currents_commit<<<1, 1, 0, s>>>(a);
     T.mark(s, KC_CURRENT, 2);
   }
-  launch_horizon(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
-  T.mark(s, KC_HORIZON);
-  k_dt_finalize<<<1, 1024, 0, s>>>(a);
+  // horizon accounting and the new dt
+  launch_step_end(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
   T.mark(s, KC_DT);
   return cudaGetLastError() == cudaSuccess ? HARM_OK : HARM_ECUDA;
 }
@@ -313,6 +317,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   if (cfg->eom != HARM_EOM_GRMHD && cfg->eom != HARM_EOM_FFDE) return HARM_EINVAL;
   if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
   if ((cfg->tryagain != 0 && cfg->tryagain != 1) || (cfg->tryagain && cfg->eom != HARM_EOM_GRMHD)) return HARM_EINVAL;
+  if (cfg->fluxadjust < 0 || cfg->fluxadjust > 3 || (cfg->fluxadjust && !(cfg->gammadamp > 0.0))) return HARM_EINVAL;
   int dev = 0, ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HARM_ENODEVICE;
   CK(cudaGetDevice(&dev));
@@ -352,6 +357,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   ok &= cudaMalloc(&c->d_pflag, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_bsqf, (size_t)c->gr.plane) == cudaSuccess;
   ok &= cudaMalloc(&c->d_chk, 2 * (size_t)c->gr.plane) == cudaSuccess;
+  if (cfg->fluxadjust) ok &= cudaMalloc(&c->d_fluxf, (size_t)c->gr.plane) == cudaSuccess;
   ok &= cudaMalloc(&c->d_sc, sizeof(DevScalars)) == cudaSuccess;
   ok &= cudaMalloc(&c->d_ubuf, NPR * pd) == cudaSuccess;
   ok &= cudaMalloc(&c->d_worklist, (size_t)c->gr.plane * sizeof(int)) == cudaSuccess;
@@ -373,6 +379,7 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   cudaMemsetAsync(c->d_pflag, 0, (size_t)c->gr.plane * sizeof(int), c->stream);
   cudaMemsetAsync(c->d_bsqf, 0, (size_t)c->gr.plane, c->stream);
   cudaMemsetAsync(c->d_chk, 0, 2 * (size_t)c->gr.plane, c->stream);
+  if (c->d_fluxf) cudaMemsetAsync(c->d_fluxf, 0, (size_t)c->gr.plane, c->stream);
   cudaMemsetAsync(c->d_sc, 0, sizeof(DevScalars), c->stream);
   if (c->d_cur) cudaMemsetAsync(c->d_cur, 0, (size_t)CUR_NPLANES * pd, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -403,6 +410,7 @@ void harm_destroy(harm_ctx* c)
   cudaFree(c->d_pflag);
   cudaFree(c->d_bsqf);
   cudaFree(c->d_chk);
+  cudaFree(c->d_fluxf);
   cudaFree(c->d_sc);
   cudaFree(c->d_ubuf);
   cudaFree(c->d_worklist);
@@ -1343,11 +1351,13 @@ static constexpr long long NA_OFF_BLOCKMIN = NA_DPLANES * NOALLOC_MAX_PLANE;
 static constexpr long long NA_OFF_SCALARS = NA_OFF_BLOCKMIN + 2 * NOALLOC_MAX_BLOCKS;
 static constexpr long long NA_OFF_WORKLIST = NA_OFF_SCALARS + 32;  // 256 B for DevScalars
 static constexpr long long NA_OFF_BYTES = NA_OFF_WORKLIST + NOALLOC_MAX_PLANE / 2;  // one int per zone
-static constexpr long long NA_DOUBLES = NA_OFF_BYTES + (3 * NOALLOC_MAX_PLANE) / 8 + 32;
+static constexpr long long NA_DOUBLES = NA_OFF_BYTES + (4 * NOALLOC_MAX_PLANE) / 8 + 32;  // bsqf, chk x2, fluxf
 static_assert(sizeof(DevScalars) <= 32 * sizeof(double), "DevScalars must fit its slot");
 static __device__ __align__(256) double g_noalloc_scratch[NA_DOUBLES];
 
 static double* g_noalloc_addr[64];  // per device: address of g_noalloc_scratch
+static int g_noalloc_arch[64];      // per device: 1 sm_100, -1 another device (checked once)
+static int g_noalloc_grid[64][3];   // per device: n1, n2 and pitch of the last call (the gamma table's layout)
 
 extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, double* d_prims, int* d_pflag, double* t,
                                  double* dt, int reset_gammacheck, void* stream)
@@ -1359,6 +1369,12 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   if (cfg->bc != HARM_BC_TORUS && cfg->bc != HARM_BC_STAR) return HARM_EINVAL;
   if (cfg->currents) return HARM_EINVAL;  // the diagnostic currents need a context
   if (cfg->tryagain != 0 && cfg->tryagain != 1) return HARM_EINVAL;
+  if (cfg->fluxadjust < 0 || cfg->fluxadjust > 3 || (cfg->fluxadjust && !(cfg->gammadamp > 0.0))) return HARM_EINVAL;
+  if (!(cfg->tf > *t)) {
+    fprintf(stderr, "harm_step_noalloc: end time tf = %g is not after t = %g (a zeroed config has tf = 0)\n", cfg->tf,
+            *t);
+    return HARM_EINVAL;
+  }
   harm_ctx c;
   memset(&c, 0, sizeof(c));
   c.cfg = *cfg;
@@ -1388,6 +1404,23 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return HARM_ENODEVICE;
+  if (!g_noalloc_arch[dev]) {
+    // the device check of harm_create (the kernels are built for sm_100a only)
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    g_noalloc_arch[dev] = (prop.major == 10) ? 1 : -1;
+  }
+  if (g_noalloc_arch[dev] < 0) return HARM_ENODEVICE;
+  {
+    // the step synchronises with the host to hand t and dt back, which a
+    // stream being captured cannot do: refuse instead of breaking the capture
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c.stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      fprintf(stderr, "harm_step_noalloc: the stream is being captured; the call must run outside a capture\n");
+      return HARM_EINVAL;
+    }
+  }
   if (!g_noalloc_addr[dev]) {
     void* p = nullptr;
     CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -1410,6 +1443,7 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.d_sc = (DevScalars*)(s + NA_OFF_SCALARS);
   c.d_bsqf = (unsigned char*)(s + NA_OFF_BYTES);
   c.d_chk = c.d_bsqf + pl;
+  c.d_fluxf = cfg->fluxadjust ? c.d_chk + 2 * pl : nullptr;
   c.geo_ok = true;
   // the array keeps the last call's contents: the run scalars start from
   // zero on every call, the check-solution gamma table only when asked
@@ -1419,7 +1453,14 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   h.dt = *dt;
   h.dt_free = *dt;
   CK(cudaMemcpyAsync(c.d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c.stream));
-  if (reset_gammacheck) CK(cudaMemsetAsync(c.d_gammacheck, 0, (size_t)pl * sizeof(double), c.stream));
+  // the gamma table left by the previous call is laid out for that call's
+  // grid: on another grid it starts from zero, as on a fresh table
+  const bool regrid = g_noalloc_grid[dev][0] != cfg->n1 || g_noalloc_grid[dev][1] != cfg->n2 ||
+                      g_noalloc_grid[dev][2] != c.gr.pitch;
+  if (reset_gammacheck || regrid) CK(cudaMemsetAsync(c.d_gammacheck, 0, (size_t)pl * sizeof(double), c.stream));
+  g_noalloc_grid[dev][0] = cfg->n1;
+  g_noalloc_grid[dev][1] = cfg->n2;
+  g_noalloc_grid[dev][2] = c.gr.pitch;
   int rc = enqueue_step(&c);
   if (rc != HARM_OK) return rc;
   CK(cudaMemcpyAsync(&h, c.d_sc, sizeof(h), cudaMemcpyDeviceToHost, c.stream));

@@ -38,8 +38,10 @@ struct Params {
   int currents;     // 1: Faraday slots and J^mu every step
   int bc;           // 0 torus (bounds.fishmon.c), 1 rotating star (bounds.ns.c)
   int tryagain;     // 1: the UTOPRIMTRYAGAIN retry chain after a failed 2D inversion
+  int fluxadjust;   // FLUXADJUST: per-zone HLL/LAXF choice of the hydro fluxes (FLAGREALFLUX)
   double cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail, bsqorholimit, bsqoulimit, tf;
   double omegastar; // bc 1: angular frequency of the stellar surface
+  double gammadamp; // GAMMADAMP: Lorentz-factor threshold of the flux switch
 };
 
 // device-resident scalars of the run (one struct in device memory)
@@ -52,7 +54,7 @@ struct DevScalars {
   int chk_changed[8];    // per-round change flags of the check-solution sweep
   int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
   int fixups;            // zones repaired by fixup_utoprim since the last harm_set_time
-  double hz[7];          // horizon accounting of the last step (see k_horizon); hz[6]:
+  double hz[7];          // horizon accounting of the last step (see k_step_end); hz[6]:
                          // sum of dt (b^2 u^r u_t - b^r b_t) terms since the last harm_set_time
   int ndeferred;         // zones whose inversion went to the tail kernel (this substep)
   int ndeferred_total;   // same, summed since the last harm_set_time
@@ -72,6 +74,7 @@ struct StepArgs {
   double* emf;           // 1 plane
   int* pflag;            // 1 plane (FLAGUTOPRIMFAIL)
   unsigned char* bsqf;   // 1 plane: (b^2/rho flag) | (b^2/u flag) << 2
+  unsigned char* fluxf;  // 1 plane (fluxadjust only): FLAGREALFLUX of the zone, 0 LAXF or 1 HLL
   double* gammacheck;    // 1 plane, persistent
   unsigned char* chk;    // 2 planes: check-solution decisions (double buffer)
   double* fixbuf;        // 5 planes: repaired rho..u3
@@ -182,14 +185,13 @@ constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 2
 // launchers of the templated step kernels (harm_step.cu: FP64 instantiations
 // and dispatch; harm_step_mixed.cu: the mixed-precision instantiations)
 void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
-void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv);
 void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
                    const double* pb, double* pf, double c2);
-void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
+void launch_step_end(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
 void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
-void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a);
+void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv);
 void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
                          const double* pb, double* pf, double c2);
-void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv);
 
 }  // namespace harm

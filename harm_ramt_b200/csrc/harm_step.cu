@@ -20,13 +20,14 @@ namespace harm {
 
 // ---------------------------------------------------------------- flags
 // get_bsqflags, fixup.c:1197-1295 over the DQZLOOP range [-1,N1]x[-1,N2]
+// (with fluxadjust also the flux choice of each zone)
 __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
   if (i > a.gr.n1 || j > a.gr.n2) return;
   const long long z = a.gr.at(i, j);
-  if (a.pp.eom) {  // the b^2 checks are GRMHD-only (fixup.c:1214-1233)
+  if (a.pp.eom && !a.pp.fluxadjust) {  // the b^2 checks are GRMHD-only (fixup.c:1214-1233)
     a.bsqf[z] = 0;
     return;
   }
@@ -35,42 +36,22 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
   for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * a.gr.plane + z);
   Geo<double> g;
   load_geo(a, CENT, z, g);
-  State<double> q;
-  state_of(pr, g, q);
-  a.bsqf[z] = bsq_flag(a, pr, q);
-}
-
-// the same for the ring of zones one outside the active grid only (i or j
-// in {-1, N}); the first substep's k_update sets the active zones' flags
-__global__ void k_bsqflags_ring(StepArgs a, const double* __restrict__ pv)
-{
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n1 = a.gr.n1, n2 = a.gr.n2;
-  int i, j;
-  if (t < n1 + 2) {
-    i = t - 1;
-    j = -1;
-  } else if (t < 2 * (n1 + 2)) {
-    i = t - (n1 + 2) - 1;
-    j = n2;
-  } else if (t < 2 * (n1 + 2) + n2) {
-    i = -1;
-    j = t - 2 * (n1 + 2);
-  } else if (t < 2 * (n1 + 2) + 2 * n2) {
-    i = n1;
-    j = t - 2 * (n1 + 2) - n2;
-  } else {
-    return;
+  unsigned char b = 0;
+  if (!a.pp.eom) {
+    State<double> q;
+    state_of(pr, g, q);
+    b = bsq_flag(a, pr, q);
   }
-  const long long z = a.gr.at(i, j);
-  double pr[NPR];
-#pragma unroll
-  for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * a.gr.plane + z);
-  Geo<double> g;
-  load_geo(a, CENT, z, g);
-  State<double> q;
-  state_of(pr, g, q);
-  a.bsqf[z] = bsq_flag(a, pr, q);
+  a.bsqf[z] = b;
+  if (a.pp.fluxadjust) {
+    // FLAGREALFLUX (fixup.c:1236-1245, 1284-1290): the Lorentz-factor flag
+    // joins the b^2 flags; where any is 2 the hydro fluxes step down from
+    // fluxmethod (HLL -> LAXF, not below LAXF)
+    const double gamma = gamma_of(pr, g);
+    const int f1 = (gamma > 2.0 * a.pp.gammadamp) ? 2 : ((gamma > a.pp.gammadamp) ? 1 : 0);
+    const int rf = ((b & 3) == 2 || f1 == 2 || (b >> 2) == 2) ? a.pp.fluxmethod - 1 : a.pp.fluxmethod;
+    a.fluxf[z] = (unsigned char)(rf < 0 ? 0 : rf);
+  }
 }
 
 // The deferred inversions of k_update, redone with the full iteration limit.
@@ -171,11 +152,28 @@ __device__ __forceinline__ int inflow_check_x1(const StepArgs& a, int i, double*
   return 0;
 }
 
+// A value of an active zone as the second bound_prim of a substep reads it
+// when the repairs of fixup_utoprim are applied in the same kernel (APPLY):
+// a repaired zone's rho..u~3 come from the repair buffer (the zone's own
+// thread writes them to pv in that kernel), everything else from pv.
+// Repaired = a failed inversion or a check-solution decision (the zones
+// k_fixup_compute wrote), or PF_FIXED once the zone's thread has marked it.
+template <bool APPLY>
+__device__ __forceinline__ double srcv(const StepArgs& a, const double* pv, long long zs, int k)
+{
+  const long long pl = a.gr.plane;
+  if (APPLY && k <= U3) {
+    if (a.pflag[zs] != 0 || a.chk[(long long)(a.sc->chk_final & 1) * pl + zs] != 0) return a.fixbuf[k * pl + zs];
+  }
+  return pv[k * pl + zs];
+}
+
 // x1 ghost zone (i, j) of the rotating star, bounds.ns.c:96-203 (NSSURFACE)
 // and 207-271 (OUTFLOW), EXTRAP 1: densities scaled by sqrt(-g); inside, the
 // velocity of the surface rotating at omegastar (vcon2pr -> ucon_calc_3vel;
 // left as it was if that fails) and the field of the step's p; outside,
 // linear extrapolation factors in x1
+template <bool APPLY>
 __device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* pv, int i, int j, double* pr)
 {
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
@@ -183,7 +181,7 @@ __device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* p
   const long long zr = a.gr.at(ri, j);
   const double gr_ = gdet_at(a, CENT, zr), gi = gdet_at(a, CENT, z);
 #pragma unroll
-  for (int k = RHO; k <= UU; k++) pr[k] = pv[k * pl + zr] * gr_ / gi;
+  for (int k = RHO; k <= UU; k++) pr[k] = srcv<APPLY>(a, pv, zr, k) * gr_ / gi;
   if (i < 0) {
     Geo<double> g;
     load_geo(a, CENT, z, g);
@@ -201,9 +199,9 @@ __device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* p
     for (int k = B1; k <= B3; k++) pr[k] = a.pstep[k * pl + z];
   } else {
     const double dx1 = a.pp.dx1;
-    pr[U1] = pv[U1 * pl + zr] * (1. - 2 * (i - ri) * dx1);
+    pr[U1] = srcv<APPLY>(a, pv, zr, U1) * (1. - 2 * (i - ri) * dx1);
 #pragma unroll
-    for (int k = U2; k <= U3; k++) pr[k] = pv[k * pl + zr] * (1. - (i - ri) * dx1);
+    for (int k = U2; k <= U3; k++) pr[k] = srcv<APPLY>(a, pv, zr, k) * (1. - (i - ri) * dx1);
     pr[B1] = pv[B1 * pl + zr] * gr_ / gi;
 #pragma unroll
     for (int k = B2; k <= B3; k++) pr[k] = pv[k * pl + zr] * (1. - (i - ri) * dx1);
@@ -212,15 +210,16 @@ __device__ __forceinline__ void x1_ghost_star(const StepArgs& a, const double* p
 
 // outflow copy + inflow check + gamma limit of an x1 ghost zone (i, j),
 // bounds.fishmon.c:28-60 and 192-230 (EXTRAP 0), or the star's
+template <bool APPLY>
 __device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, int i, int j, double* pr, int phase)
 {
   if (a.pp.bc == 1) {
-    x1_ghost_star(a, pv, i, j, pr);
+    x1_ghost_star<APPLY>(a, pv, i, j, pr);
   } else {
     const int is = (i < 0) ? 0 : a.gr.n1 - 1;
     const long long zs = a.gr.at(is, j);
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pr[k] = pv[k * a.gr.plane + zs];
+    for (int k = 0; k < NPR; k++) pr[k] = srcv<APPLY>(a, pv, zs, k);
   }
   Geo<double> g;
   load_geo(a, CENT, a.gr.at(i, j), g);
@@ -235,20 +234,17 @@ __device__ __forceinline__ void x1_ghost(const StepArgs& a, const double* pv, in
 // the x1 ghost value of their mirror row, as the reference's x1-then-x2 order
 // produces.  The torus's POLEDEATH rows are zeroed here for ghost zones and
 // by k_poledeath for the first and last active rows.
-__global__ void k_bound(StepArgs a, double* pv, int with_pflag)
+template <bool APPLY>
+__device__ __forceinline__ void bound_ghost(const StepArgs& a, double* pv, int i, int j, int with_pflag)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
-  if (i >= n1 + NG || j >= n2 + NG) return;
   const bool xin = (i >= 0 && i < n1), yin = (j >= 0 && j < n2);
-  if (xin && yin) return;
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
   double pr[NPR];
   const bool poledeath = (a.pp.bc == 0);
   const int phase = a.phase0 + (with_pflag ? PH_BOUND1 : PH_BOUND2);
   if (yin) {
-    x1_ghost(a, pv, i, j, pr, phase);
+    x1_ghost<APPLY>(a, pv, i, j, pr, phase);
     if (poledeath && (j == 0 || j == n2 - 1)) {
       pr[U2] *= 0.;
       pr[B2] *= 0.;
@@ -258,9 +254,9 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
     if (xin) {
       const long long zs = a.gr.at(i, jm);
 #pragma unroll
-      for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + zs];
+      for (int k = 0; k < NPR; k++) pr[k] = srcv<APPLY>(a, pv, zs, k);
     } else {
-      x1_ghost(a, pv, i, jm, pr, phase);
+      x1_ghost<APPLY>(a, pv, i, jm, pr, phase);
     }
     if (poledeath) {
       pr[U2] *= 0.;
@@ -274,6 +270,52 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
     const int js = (j < 0) ? (-j - 1) : ((j >= n2) ? (2 * n2 - 1 - j) : j);
     a.pflag[z] = a.pflag[a.gr.at(is, js)];
   }
+}
+
+__global__ void k_bound(StepArgs a, double* pv, int with_pflag)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (i >= n1 + NG || j >= n2 + NG) return;
+  if (i >= 0 && i < n1 && j >= 0 && j < n2) return;
+  bound_ghost<false>(a, pv, i, j, with_pflag);
+}
+
+// The end of a GRMHD substep in one kernel: fixup_utoprim's repairs applied
+// (the zones k_fixup_compute repaired take their rho..u~3 from the repair
+// buffer and are flagged PF_FIXED, fixup.c:527-928), the second bound_prim
+// (bounds.fishmon.c:14-330; the ghost zones read a repaired zone's values
+// from the repair buffer, so they see the repaired state whichever thread
+// runs first) and its POLEDEATH zeroing of u~2 and B2 on the first and last
+// active rows (bounds.fishmon.c:296-327).  The zeroing comes after the
+// ghosts have read those rows in the reference: a zone there that was not
+// repaired holds u~2 = B2 = 0 already (the first bound zeroed them and
+// nothing changed them since), so the ghosts read the same value before or
+// after it is rewritten; a repaired one is read from the repair buffer.
+__global__ void k_bound_fix(StepArgs a, double* pv)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (i >= n1 + NG || j >= n2 + NG) return;
+  if (i >= 0 && i < n1 && j >= 0 && j < n2) {
+    const long long pl = a.gr.plane, z = a.gr.at(i, j);
+    const int f = a.pflag[z];
+    const int c = a.chk[(long long)(a.sc->chk_final & 1) * pl + z];
+    if (f != 0 || c != 0) {
+#pragma unroll
+      for (int k = 0; k <= U3; k++) pv[k * pl + z] = a.fixbuf[k * pl + z];
+      a.pflag[z] = PF_FIXED;
+      atomicAdd(&a.sc->fixups, 1);
+    }
+    if (a.pp.bc == 0 && (j == 0 || j == n2 - 1)) {
+      pv[U2 * pl + z] *= 0.;
+      pv[B2 * pl + z] *= 0.;
+    }
+    return;
+  }
+  bound_ghost<true>(a, pv, i, j, 0);
 }
 
 // POLEDEATH on the first and last active x2 rows (bounds.fishmon.c:296-327)
@@ -514,58 +556,6 @@ __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd)
   }
 }
 
-// ---------------------------------------------------------------- dt
-// advance.c:190 and step_ch.c:174-183, after the last substep
-__global__ void k_dt_finalize(StepArgs a)
-{
-  __shared__ double sh[2][32];
-  __shared__ double acc[4];
-  __shared__ double buf[4][256];
-  // the horizon sums of k_horizon's per-j terms, in j order (diag.c:576-833):
-  // the block stages 256 j at a time in shared memory, four threads add
-  if (threadIdx.x < 4) acc[threadIdx.x] = 0.;
-  for (int j0 = 0; j0 < a.gr.n2; j0 += 256) {
-    const int m = (a.gr.n2 - j0 < 256) ? a.gr.n2 - j0 : 256;
-    const int k = threadIdx.x >> 8, jj = threadIdx.x & 255;
-    if (k < 4 && jj < m) buf[k][jj] = a.fixbuf[(long long)k * a.gr.plane + j0 + jj];
-    __syncthreads();
-    if (threadIdx.x < 4) {
-      double s = acc[threadIdx.x];
-      for (int q = 0; q < m; q++) s += buf[threadIdx.x][q];
-      acc[threadIdx.x] = s;
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    DevScalars* sc = a.sc;
-    for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
-    sc->hz[4] += acc[0] * sc->dt;
-    sc->hz[5] += acc[1] * sc->dt;
-    sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
-  }
-  double m1 = 1.e9, m2 = 1.e9;
-  for (int b = threadIdx.x; b < a.nblocks_flux; b += blockDim.x) {
-    double v1 = a.blockmin[b], v2 = a.blockmin[a.nblocks_flux + b];
-    m1 = (v1 < m1) ? v1 : m1;
-    m2 = (v2 < m2) ? v2 : m2;
-  }
-  m1 = block_min(m1, sh[0]);
-  m2 = block_min(m2, sh[1]);
-  if (threadIdx.x == 0) {
-    DevScalars* s = a.sc;
-    double ndt = a.pp.defcon * 1. / (1. / m1 + 1. / m2);
-    s->ndt = ndt;
-    const bool moved = s->dt > 0.;
-    s->t += s->dt;
-    s->realnstep += 1;
-    if (ndt > a.pp.safe * s->dt) ndt = a.pp.safe * s->dt;
-    s->dt = ndt;
-    if (moved) s->dt_free = ndt;  // a step at dt = 0 (past the end time) keeps the last one
-    if (s->t + s->dt > a.pp.tf) s->dt = a.pp.tf - s->t;
-  }
-}
-
 // ---------------------------------------------------------------- currents
 // current_doprecalc(0..3, p) with WHICHCURRENTCALC 1 (phys.c:1124-1218): at
 // every zone centre (ghosts included) the F^{i t} components go to the next
@@ -799,7 +789,9 @@ __global__ void k_planes_to_ref(StepArgs a, const double* __restrict__ pv, doubl
     f[1] = 0;
     f[2] = b & 3;
     f[3] = (b >> 2) & 3;
-    f[4] = 0;
+    // FLAGREALFLUX where get_bsqflags sets it (the DQZLOOP range)
+    const int i = ii - NG, j = jj - NG;
+    f[4] = (a.fluxf && i >= -1 && i <= a.gr.n1 && j >= -1 && j <= a.gr.n2) ? (int)a.fluxf[zd] : 0;
   }
 }
 
@@ -816,10 +808,10 @@ void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, 
   else flux_rows_launch<double, false, false>(g, b, s, a, pb);
 }
 
-void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a)
+void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv)
 {
-  if (mixed) launch_emf_mixed(g, b, s, a);
-  else k_emf<double><<<g, b, 0, s>>>(a);
+  if (mixed) launch_emf_mixed(g, b, s, a, pv);
+  else k_emf<double><<<g, b, 0, s>>>(a, pv);
 }
 
 void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
@@ -834,10 +826,12 @@ void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const St
   }
 }
 
-void launch_horizon(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)
+// both instances here: the horizon sums and the new dt are FP64 work built
+// without contraction in either precision
+void launch_step_end(int mixed, cudaStream_t s, const StepArgs& a, const double* pv)
 {
-  if (mixed) launch_horizon_mixed(s, a, pv);
-  else k_horizon<double><<<(a.gr.n2 + 63) / 64, 64, 0, s>>>(a, pv);
+  if (mixed) k_step_end<float><<<1, STEP_END_THREADS, 0, s>>>(a, pv);
+  else k_step_end<double><<<1, STEP_END_THREADS, 0, s>>>(a, pv);
 }
 
 }  // namespace harm

@@ -71,13 +71,19 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   lmin = fabs(rmax(T(0.), -lmin));
   lmax = fabs(rmax(T(0.), lmax));
   T cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
-  const T hllfrac = (a.pp.fluxmethod == 1) ? T(1.0) : T(0.0);
-  const T laxffrac = (a.pp.fluxmethod == 1) ? T(0.0) : T(1.0);
+  // choose_flux, step_ch.c:703-738: fluxmethod, or with FLUXADJUST
+  // (HYDROFLUXADJUSTONLY 1) the hydro variables follow FLAGREALFLUX of zone
+  // (i, j), the face's own zone
+  const int rf = a.pp.fluxadjust ? (int)a.fluxf[z] : a.pp.fluxmethod;
+  const T hll_h = (rf == 1) ? T(1.0) : T(0.0), laxf_h = (rf == 1) ? T(0.0) : T(1.0);
+  const T hll_b = (a.pp.fluxmethod == 1) ? T(1.0) : T(0.0), laxf_b = (a.pp.fluxmethod == 1) ? T(0.0) : T(1.0);
   if (cmax + cmin != T(0.0)) {
 #pragma unroll
-    for (int k = 0; k < NPR; k++)
+    for (int k = 0; k < NPR; k++) {
+      const T hllfrac = (k < B1) ? hll_h : hll_b, laxffrac = (k < B1) ? laxf_h : laxf_b;
       Fo[k] = hllfrac * ((cmax * F_l[k] + cmin * F_r[k] - cmax * cmin * (U_r[k] - U_l[k])) / (cmax + cmin)) +
               laxffrac * (T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k])));
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < NPR; k++) Fo[k] = T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k]));
@@ -197,14 +203,31 @@ inline void flux_rows_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, 
 
 // flux_ct corner EMF, step_ch.c:1214-1234, over i in [0,N1], j in [0,N2].
 // F1 on the rows j = -1 and j = N2 carries fix_flux's mirrored B2 for i < N1.
+// The grid spans i, j from -1: with bsqf_fused set (the first substep of an
+// FP64 GRMHD step) the threads of the ring one zone outside the active grid
+// (i or j in {-1, N}) set the b^2 flags of their zone from the step's p, as
+// get_bsqflags does over its DQZLOOP range (fixup.c:1197-1233); the first
+// substep's k_update sets those of the active zones.
 template <typename FT>
-__global__ void k_emf(StepArgs a)
+__global__ void k_emf(StepArgs a, const double* __restrict__ pv)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   if (i == 0 && j == 0) a.sc->ndeferred = 0;
   if (i > n1 || j > n2) return;
+  if (a.bsqf_fused && (i == -1 || i == n1 || j == -1 || j == n2)) {
+    const long long z = a.gr.at(i, j);
+    double pr[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pr[k] = __ldg(pv + k * a.gr.plane + z);
+    Geo<double> g;
+    load_geo(a, CENT, z, g);
+    State<double> q;
+    state_of(pr, g, q);
+    a.bsqf[z] = bsq_flag(a, pr, q);
+  }
+  if (i < 0 || j < 0) return;
   const long long pl = a.gr.plane;
   const FT* F1b2 = reinterpret_cast<const FT*>(a.F1) + B2 * pl;
   const FT* F2b1 = reinterpret_cast<const FT*>(a.F2) + B1 * pl;
@@ -360,20 +383,14 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
 
 
 
-// ---------------------------------------------------------------- horizon
+// ---------------------------------------------------------------- end of step
 // diag_flux() for the global region's inner x1 face (diag.c:576-833): the
 // face fluxes in diagnostic form (UtoU UEVOLVE->UDIAG) and the energy-
-// equation stress terms 3 and 6 from the zone-centred state, per j, in
-// parallel, into the repair scratch (idle at this point of the step):
-// fixbuf[k * plane + j], k = 0..3.  k_dt_finalize then sums them in j order,
-// as the reference's loop does (so the sums are exact), and adds pcum +=
-// pdot * dt.
+// equation stress terms 3 and 6 from the zone-centred state of row j.
 template <typename FT>
-__global__ void __launch_bounds__(64) k_horizon(StepArgs a, const double* __restrict__ pv)
+__device__ __forceinline__ void horizon_terms(const StepArgs& a, const double* __restrict__ pv, int j, double* t4)
 {
   const FT* F1 = reinterpret_cast<const FT*>(a.F1);
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.gr.n2) return;
   const long long pl = a.gr.plane;
   const double surface = a.pp.dx2 * (2.0 * 3.14159265358979323846);
   const long long z = a.gr.at(0, j);
@@ -382,9 +399,8 @@ __global__ void __launch_bounds__(64) k_horizon(StepArgs a, const double* __rest
   const double gr = Fr / gf;
   double gu = Fu / gf;
   gu += -gr;
-  double* t = a.fixbuf;
-  t[j] = gr * gf;
-  t[pl + j] = gu * gf;
+  t4[0] = gr * gf;
+  t4[1] = gu * gf;
   double pr[NPR];
 #pragma unroll
   for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
@@ -396,8 +412,65 @@ __global__ void __launch_bounds__(64) k_horizon(StepArgs a, const double* __rest
 #pragma unroll
   for (int l = 0; l < 4; l++) bsq += (q.bcon[l]) * (q.bcov[l]);
   const double surgdet = (g.g) * surface;
-  t[2 * pl + j] = bsq * (q.ucon[1]) * (q.ucov[0]) * surgdet;
-  t[3 * pl + j] = -(q.bcon[1]) * (q.bcov[0]) * surgdet;
+  t4[2] = bsq * (q.ucon[1]) * (q.ucov[0]) * surgdet;
+  t4[3] = -(q.bcon[1]) * (q.bcov[0]) * surgdet;
+}
+
+// After the last substep, one block: the horizon terms of every row j, their
+// sums in j order as the reference's loop adds them (so the sums are exact),
+// pcum += pdot * dt (diag.c:576-833); then the new dt from the flux blocks'
+// Courant minima (advance.c:190, step_ch.c:174-183) and t += dt.
+constexpr int STEP_END_THREADS = 1024;
+template <typename FT>
+__global__ void __launch_bounds__(STEP_END_THREADS) k_step_end(StepArgs a, const double* __restrict__ pv)
+{
+  __shared__ double sh[2][32];
+  __shared__ double acc[4];
+  __shared__ double buf[4][STEP_END_THREADS];
+  if (threadIdx.x < 4) acc[threadIdx.x] = 0.;
+  for (int j0 = 0; j0 < a.gr.n2; j0 += STEP_END_THREADS) {
+    const int m = (a.gr.n2 - j0 < STEP_END_THREADS) ? a.gr.n2 - j0 : STEP_END_THREADS;
+    if ((int)threadIdx.x < m) {
+      double t4[4];
+      horizon_terms<FT>(a, pv, j0 + threadIdx.x, t4);
+#pragma unroll
+      for (int k = 0; k < 4; k++) buf[k][threadIdx.x] = t4[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double s = acc[threadIdx.x];
+      for (int q = 0; q < m; q++) s += buf[threadIdx.x][q];
+      acc[threadIdx.x] = s;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    DevScalars* sc = a.sc;
+    for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
+    sc->hz[4] += acc[0] * sc->dt;
+    sc->hz[5] += acc[1] * sc->dt;
+    sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
+  }
+  double m1 = 1.e9, m2 = 1.e9;
+  for (int b = threadIdx.x; b < a.nblocks_flux; b += blockDim.x) {
+    double v1 = a.blockmin[b], v2 = a.blockmin[a.nblocks_flux + b];
+    m1 = (v1 < m1) ? v1 : m1;
+    m2 = (v2 < m2) ? v2 : m2;
+  }
+  m1 = block_min(m1, sh[0]);
+  m2 = block_min(m2, sh[1]);
+  if (threadIdx.x == 0) {
+    DevScalars* s = a.sc;
+    double ndt = a.pp.defcon * 1. / (1. / m1 + 1. / m2);
+    s->ndt = ndt;
+    const bool moved = s->dt > 0.;
+    s->t += s->dt;
+    s->realnstep += 1;
+    if (ndt > a.pp.safe * s->dt) ndt = a.pp.safe * s->dt;
+    s->dt = ndt;
+    if (moved) s->dt_free = ndt;  // a step at dt = 0 (past the end time) keeps the last one
+    if (s->t + s->dt > a.pp.tf) s->dt = a.pp.tf - s->t;
+  }
 }
 
 }  // namespace harm

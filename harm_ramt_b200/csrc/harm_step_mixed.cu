@@ -17,18 +17,16 @@ void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const
   else flux_rows_launch<float, false, false>(g, b, s, a, pb);
 }
 
-void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a) { k_emf<float><<<g, b, 0, s>>>(a); }
+void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv)
+{
+  k_emf<float><<<g, b, 0, s>>>(a, pv);
+}
 
 void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
                          const double* pb, double* pf, double c2)
 {
   if (ffde) k_update<float, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
   else k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
-}
-
-void launch_horizon_mixed(cudaStream_t s, const StepArgs& a, const double* pv)
-{
-  k_horizon<float><<<(a.gr.n2 + 63) / 64, 64, 0, s>>>(a, pv);
 }
 
 }  // namespace harm

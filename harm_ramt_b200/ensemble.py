@@ -32,7 +32,7 @@ def _setup(hb, spec):
     return par, geom, p0
 
 
-def build(hb, specs, *, lim, fluxmethod, precision=0, stream=None, threads=16):
+def build(hb, specs, *, lim, fluxmethod, precision=0, stream=None, threads=16, fluxadjust=0):
     """One context per spec, uploaded, bounded and at t = 0 (dt = 1e-5), with
     (params, geometry, initial prims) kept for restarting."""
     with ThreadPoolExecutor(max_workers=threads) as ex:
@@ -40,7 +40,7 @@ def build(hb, specs, *, lim, fluxmethod, precision=0, stream=None, threads=16):
     members = []
     for spec, (par, geom, p0) in zip(specs, made):
         h = hb.HarmGPU(spec["n1"], spec["n2"], geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, gam=par.gam,
-                       gammamax=par.gammamax, precision=precision, stream=stream)
+                       gammamax=par.gammamax, precision=precision, stream=stream, fluxadjust=fluxadjust)
         h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
         h.set_prims(p0)
         h.bound_prims()

@@ -86,7 +86,8 @@ typedef struct harm_config {
   double gammafail;     /* GAMMAFAIL */
   double bsqorholimit;  /* BSQORHOLIMIT */
   double bsqoulimit;    /* BSQOULIMIT */
-  double tf;            /* end time: dt is clamped so that t + dt <= tf */
+  double tf;            /* end time: dt is clamped so that t + dt <= tf (a zeroed
+                           config has tf = 0, which stops a run at t = 0) */
   int bc;               /* HARM_BC_TORUS or HARM_BC_STAR */
   double omegastar;     /* HARM_BC_STAR: angular frequency of the surface
                            (Omegastar, bounds.ns.c:107) */
@@ -98,6 +99,18 @@ typedef struct harm_config {
                            is inverted again by 5D1, 2D, 1D, 1D_OPT, 1D_FINAL,
                            2D_FINAL and 5D2_FINAL in turn until one succeeds;
                            0: the 2D inversion only (GRMHD only) */
+  int fluxadjust;       /* FLUXADJUST (global.h:286-293): 0 FLUXFIXED, every face
+                           uses fluxmethod; 1 FLUXBSQORHO, 2 FLUXBSQOU, 3
+                           FLUXBSQORHOANDU: per zone, the hydro variables of
+                           the faces a zone owns switch one step down from
+                           fluxmethod (HLL -> LAXF) where b^2/rho >
+                           bsqorholimit, b^2/u > bsqoulimit or the Lorentz
+                           factor > 2 gammadamp (get_bsqflags' FLAGREALFLUX,
+                           fixup.c:1236-1290; choose_flux with
+                           HYDROFLUXADJUSTONLY 1, step_ch.c:703-738).  The
+                           reference decides alike for 1, 2 and 3. */
+  double gammadamp;     /* GAMMADAMP (initbase.c:215 sets 5.0); read only when
+                           fluxadjust != 0, and must then be > 0 */
 } harm_config;
 
 typedef struct harm_status {
@@ -290,6 +303,13 @@ int harm_run_fixed_dt(harm_ctx* ctx, const double* dts, int nsteps, double w_mas
 int harm_profile_step(harm_ctx* ctx, double* ms, int* launches, int nclasses);
 const char* harm_kernel_name(int k);
 
+/* Diagnostics: the device's FP64 instruction throughput (DADD, DMUL and
+   DFMA per second, out3[0..2]) from independent dependency chains on every
+   SM, timed with CUDA events -- the compute ceiling of the FP64 step, whose
+   kernels are built without multiply-add contraction.  No counterpart in
+   the reference. */
+int harm_measure_fp64_peak(double* out3);
+
 /* One step of step_ch() that allocates nothing -- no counterpart in the
    reference.  For callers that cannot call cudaMalloc (a host code that owns
    all device memory through its own pool, or that runs where allocation is
@@ -306,12 +326,17 @@ const char* harm_kernel_name(int k);
    for loc = FACE1, FACE2, CORN, CENT 10 gcov + 10 gcon (packed symmetric,
    00 01 02 03 11 12 13 22 23 33) + gdet, then 40 connection planes
    Gamma^k_{(lj)} (k*10 + packed (l,j)), then the rho and u floors.
-   t and dt are host values, advanced as step_ch() does.  The first call on
-   a device looks up the array's device address (cudaGetSymbolAddress), so
-   make it before any stream capture.  Every call shares the one array:
-   calls that overlap on the GPU race.  The fixup_checksolution gamma table
-   (static in the reference, fixup.c:393) carries over between calls unless
-   reset_gammacheck != 0.  Only cfg->precision == HARM_PREC_FP64. */
+   t and dt are host values, advanced as step_ch() does; cfg->tf must be
+   after *t.  The first call on a device checks that it is an sm_100 device
+   (else HARM_ENODEVICE) and looks up the array's device address
+   (cudaGetSymbolAddress).  Every call waits for its stream to hand t and dt
+   back, so no call may be made while its stream is being captured into a
+   CUDA graph (such a call returns HARM_EINVAL and leaves the capture
+   intact).  Every call shares the one array: calls that overlap on the GPU
+   race.  The fixup_checksolution gamma table (static in the reference,
+   fixup.c:393) carries over between calls on the same grid unless
+   reset_gammacheck != 0; a call on a grid other than the previous call's
+   starts it from zero.  Only cfg->precision == HARM_PREC_FP64. */
 int harm_step_noalloc(const harm_config* cfg, const double* d_geo, double* d_prims, int* d_pflag, double* t,
                       double* dt, int reset_gammacheck, void* stream);
 

@@ -44,6 +44,12 @@ Build patches (each one asserted to apply exactly):
  13. compiled -O2 -ffp-contract=off -fno-fast-math so that no FMA
      contraction changes the FP64 rounding.
 
+The "torusfa" problem is the torus with the per-zone HLL/LAXF switch of
+the benchmark's larger configurations: global.h:292 FLUXADJUST FLUXFIXED ->
+FLUXBSQORHOANDU (the alternative line 293 carries), so get_bsqflags sets
+pflag[FLAGREALFLUX] (fixup.c:1284-1290) and choose_flux follows it
+(step_ch.c:703-738).
+
 The "torusta" problem is the torus with the UTOPRIMTRYAGAIN chain on
 (step_ch.c:608-626), the build that pins the retry chain.  It differs from
 "torus" in three patches:
@@ -83,6 +89,10 @@ PROBLEMS = {
     # the same with the UTOPRIMTRYAGAIN retry chain of inversions on
     "torusta": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c",
                     defs=["-DHR_TRYAGAIN"], tryagain=True),
+    # the torus with the per-zone HLL/LAXF switch: FLUXADJUST FLUXBSQORHOANDU
+    # (the alternative global.h:293 keeps commented out), HYDROFLUXADJUSTONLY 1
+    "torusfa": dict(eom="EOMGRMHD", mcoord="KSCOORDS", init="init.fishmon.c", bounds="bounds.fishmon.c", defs=[],
+                    fluxadjust=True),
     # Force-free aligned rotator (dipole field, rotating stellar surface) in
     # flat space, spherical polar log-r coordinates (FFDE).
     "dipole": dict(eom="EOMFFDE", mcoord="SPCMINKMETRIC", init="init.ns.c", bounds="bounds.ns.c",
@@ -123,6 +133,8 @@ def patch_tree(bdir, problem, n1, n2):
         t = sub1(t, "#define EOMTYPE EOMFFDE", f"#define EOMTYPE {prob['eom']}", f)
         if not prob.get("tryagain"):
             t = sub1(t, "#define UTOPRIMTRYAGAIN 1", "#define UTOPRIMTRYAGAIN 0", f)
+        if prob.get("fluxadjust"):
+            t = sub1(t, "#define FLUXADJUST FLUXFIXED", "#define FLUXADJUST FLUXBSQORHOANDU", f)
         t = sub1(t, "#define MAILWHENDONE 1", "#define MAILWHENDONE 0", f)
         t = sub1(t, "#define PRODUCTION 0", "#define PRODUCTION 1", f)
         return t
@@ -219,6 +231,65 @@ def build(src, problem, n1, n2, jobs, force=False):
     return lib
 
 
+NATIVE_CFLAGS = ["-O3", "-march=native", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-fPIC", "-w",
+                 "-std=gnu99"]
+
+
+def _host_cpu():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def build_native(problem, n1, n2, jobs):
+    """The CPU baseline: the already patched scratch tree of a build
+    (oracle/_ref/build/<problem>_<N1>x<N2>, which the parity build left
+    behind) compiled -O3 -march=native -ffp-contract=off for the host this
+    runs on, into oracle/_ref/native/.  Rebuilt when the host CPU model
+    differs from the one the library was built for.  Needs no reference
+    tree (it may run where only the scratch tree was carried)."""
+    tag = f"{problem}_{n1}x{n2}"
+    bdir = os.path.join(OUT, "build", tag)
+    if not os.path.isdir(bdir):
+        raise SystemExit(f"no scratch tree {bdir}: run the parity build of {tag} first")
+    ndir = os.path.join(OUT, "native")
+    os.makedirs(ndir, exist_ok=True)
+    lib = os.path.join(ndir, f"libharmref_{tag}.so")
+    stamp = lib + ".cpu"
+    cpu = _host_cpu()
+    if os.path.exists(lib) and os.path.exists(stamp):
+        with open(stamp) as f:
+            if f.read() == cpu:
+                return lib
+    odir = os.path.join(ndir, "obj_" + tag)
+    os.makedirs(odir, exist_ok=True)
+    srcs = BASE_SRCS + (TRYAGAIN_SRCS if PROBLEMS[problem].get("tryagain") else []) + ["hr_harness.c"]
+
+    def cc(name):
+        obj = os.path.join(odir, name[:-2] + ".o")
+        cmd = ["gcc"] + NATIVE_CFLAGS + PROBLEMS[problem]["defs"] + ["-c", os.path.join(bdir, name), "-o", obj]
+        r = subprocess.run(cmd, cwd=bdir, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"compile failed: {name}\n{r.stderr[-3000:]}")
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(cc, srcs))
+    tmp = lib + ".tmp%d" % os.getpid()
+    r = subprocess.run(["gcc", "-shared", "-Wl,-Bsymbolic", "-o", tmp] + objs + ["-lm"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed\n" + r.stderr[-3000:])
+    os.replace(tmp, lib)
+    with open(stamp, "w") as f:
+        f.write(cpu)
+    return lib
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--src", default=os.environ.get("HARM_REFERENCE_SRC", "/root/reference"),
@@ -227,7 +298,14 @@ def main():
     ap.add_argument("--sizes", default="16x16,32x32,64x64,128x128")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--native", action="store_true",
+                    help="compile the existing scratch tree -O3 -march=native for this host (the CPU baseline)")
     a = ap.parse_args()
+    if a.native:
+        for sz in a.sizes.split(","):
+            n1, n2 = (int(v) for v in sz.split("x"))
+            print(build_native(a.problem, n1, n2, a.jobs))
+        return 0
     if not os.path.isdir(a.src):
         print(f"reference tree {a.src} not present; nothing built", file=sys.stderr)
         return 0

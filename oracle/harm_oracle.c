@@ -41,7 +41,7 @@
 #define NFL 5
 enum { RHO = 0, UU, U1, U2, U3, B1, B2, B3 };
 enum { FACE1 = 0, FACE2 = 1, CORN = 2, CENT = 3 };
-enum { F_FAIL = 0, F_BSQORHO = 2, F_BSQOU = 3 };
+enum { F_FAIL = 0, F_BSQORHO = 2, F_BSQOU = 3, F_REALFLUX = 4 };
 enum { LIM_MC = 3, LIM_PARA = 4 };
 enum { FLUX_LAXF = 0, FLUX_HLL = 1 };
 
@@ -87,6 +87,7 @@ struct ho_state {
   double hz[6];       /* horizon accounting, see ho_get_horizon */
   double dt_free;     /* the last step's next dt before the end-time clamp */
   const double *pcur; /* the step's p (bounds.ns.c reads the global p's field) */
+  const int *pfcur;   /* the step's pflag (fluxcalc reads FLAGREALFLUX) */
   double *cfar;       /* current_precalc slots, [n1m][n2m][5][3] like cfaraday */
   double *fcon;       /* [n1m][n2m][6] */
   double *jcon;       /* [n1m][n2m][4] */
@@ -458,13 +459,19 @@ static int fluxcalc(ho_state *s, const double *pb, double *F, int dir, double *n
       lmin = fabs(rmax(0., -lmin));
       lmax = fabs(rmax(0., lmax));
       double cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
-      double hllfrac = (s->c.fluxmethod == FLUX_HLL) ? 1.0 : 0.0;
-      double laxffrac = (s->c.fluxmethod == FLUX_HLL) ? 0.0 : 1.0;
+      /* choose_flux, step_ch.c:703-738: with FLUXADJUST and
+         HYDROFLUXADJUSTONLY 1 the hydro variables follow FLAGREALFLUX of
+         zone (i, j), the field ones fluxmethod */
+      const int rf = s->c.fluxadjust ? FL(s->pfcur, i, j)[F_REALFLUX] : s->c.fluxmethod;
       double *Fo = P(F, i, j);
       if (cmax + cmin != 0.0) {
-        for (k = 0; k < NPR; k++)
+        for (k = 0; k < NPR; k++) {
+          const int m = (k < B1) ? rf : s->c.fluxmethod;
+          const double hllfrac = (m == FLUX_HLL) ? 1.0 : 0.0;
+          const double laxffrac = (m == FLUX_HLL) ? 0.0 : 1.0;
           Fo[k] = hllfrac * ((cmax * F_l[k] + cmin * F_r[k] - cmax * cmin * (U_r[k] - U_l[k])) / (cmax + cmin)) +
                   laxffrac * (0.5 * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k])));
+        }
       } else {
         for (k = 0; k < NPR; k++) Fo[k] = (0.5 * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k])));
       }
@@ -921,22 +928,28 @@ static void bsqflags(ho_state *s, const double *pv, int *pf)
       geo g = getgeo(s, i, j, CENT);
       ostate q;
       const double *pr = P(pv, i, j);
-      int f0, f3;
-      if (s->c.eom) { /* the b^2 checks are GRMHD-only (fixup.c:1214-1233) */
-        FL(pf, i, j)[F_BSQORHO] = 0;
-        FL(pf, i, j)[F_BSQOU] = 0;
-        continue;
+      int f0 = 0, f3 = 0;
+      if (!s->c.eom) { /* the b^2 checks are GRMHD-only (fixup.c:1214-1233) */
+        state_of(pr, &g, &q);
+        double bsq = dot4(q.bcon, q.bcov);
+        if (bsq / pr[RHO] > s->c.bsqorholimit) f0 = 2;
+        else if (bsq / pr[RHO] > 0.9 * s->c.bsqorholimit) f0 = 1;
+        else f0 = 0;
+        if (bsq / pr[UU] > s->c.bsqoulimit) f3 = 2;
+        else if (bsq / pr[UU] > 0.9 * s->c.bsqoulimit) f3 = 1;
+        else f3 = 0;
       }
-      state_of(pr, &g, &q);
-      double bsq = dot4(q.bcon, q.bcov);
-      if (bsq / pr[RHO] > s->c.bsqorholimit) f0 = 2;
-      else if (bsq / pr[RHO] > 0.9 * s->c.bsqorholimit) f0 = 1;
-      else f0 = 0;
-      if (bsq / pr[UU] > s->c.bsqoulimit) f3 = 2;
-      else if (bsq / pr[UU] > 0.9 * s->c.bsqoulimit) f3 = 1;
-      else f3 = 0;
       FL(pf, i, j)[F_BSQORHO] = f0;
       FL(pf, i, j)[F_BSQOU] = f3;
+      if (s->c.fluxadjust) {
+        /* FLAGREALFLUX (fixup.c:1236-1245, 1284-1290): the Lorentz-factor
+           flag, then one step down from fluxmethod (HLL -> LAXF, not below
+           0) where any flag is 2 */
+        const double gamma = gamma_of(pr, &g);
+        const int f1 = (gamma > 2.0 * s->c.gammadamp) ? 2 : ((gamma > s->c.gammadamp) ? 1 : 0);
+        int rf = (f0 == 2 || f1 == 2 || f3 == 2) ? s->c.fluxmethod - 1 : s->c.fluxmethod;
+        FL(pf, i, j)[F_REALFLUX] = (rf < 0) ? 0 : rf;
+      }
     }
 }
 
@@ -1337,6 +1350,7 @@ int ho_step(ho_state *s, double *p, int *pflag, double *t, double *dt)
   double ndt = 0.0;
   int to, rc, moved;
   s->pcur = p;
+  s->pfcur = pflag;
   s->fail = s->fail_i = s->fail_j = 0;
   for (to = 0; to < 2; to++) {
     const double *pi = p;

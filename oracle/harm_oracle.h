@@ -30,6 +30,8 @@ typedef struct {
   double tf;
   int bc;              /* 0 = torus (bounds.fishmon.c), 1 = rotating star (bounds.ns.c) */
   double omegastar;    /* bc 1: angular frequency of the stellar surface */
+  int fluxadjust;      /* FLUXADJUST (global.h:286-293): 0 = FLUXFIXED, 1-3 = per-zone HLL/LAXF switch */
+  double gammadamp;    /* GAMMADAMP (initbase.c:215): Lorentz-factor threshold of the switch */
 } ho_config;
 
 typedef struct ho_state ho_state;

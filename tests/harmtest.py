@@ -27,7 +27,7 @@ class OracleConfig(ctypes.Structure):
                 ("dx2", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
                 ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("bsqorholimit", ctypes.c_double),
                 ("bsqoulimit", ctypes.c_double), ("tf", ctypes.c_double), ("bc", ctypes.c_int),
-                ("omegastar", ctypes.c_double)]
+                ("omegastar", ctypes.c_double), ("fluxadjust", ctypes.c_int), ("gammadamp", ctypes.c_double)]
 
 
 def build_oracle(force=False):
@@ -86,10 +86,10 @@ class Oracle:
 
     def __init__(self, n1, n2, geom, *, lim=3, fluxmethod=1, cour=0.8, gam=4.0 / 3.0, dx1, dx2, safe=1.3,
                  defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1e30, eom=0,
-                 bc=0, omegastar=0.0):
+                 bc=0, omegastar=0.0, fluxadjust=0, gammadamp=5.0):
         self.lib = oracle_lib()
         self.cfg = OracleConfig(n1, n2, lim, fluxmethod, eom, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
-                                bsqorholimit, bsqoulimit, tf, bc, omegastar)
+                                bsqorholimit, bsqoulimit, tf, bc, omegastar, fluxadjust, gammadamp)
         self.geom = {k: np.ascontiguousarray(geom[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "conn",
                                                                                      "floors")}
         g = self.geom
@@ -168,14 +168,18 @@ def ref_lib_path(n1, n2, problem="torus"):
     return p if os.path.exists(p) else None
 
 
-def _ref_worker(libpath, lim, flux, cour, nsteps, outpath, dump=False):
-    """Runs in a child process: reference init + nsteps steps, pickled to outpath."""
+def _ref_worker(libpath, lim, flux, cour, nsteps, outpath, dump=False, limits=None):
+    """Runs in a child process: reference init + nsteps steps, pickled to
+    outpath.  limits: (BSQORHOLIMIT, BSQOULIMIT, GAMMADAMP) or None."""
     import pickle
     lib = ctypes.CDLL(libpath)
     lib.hr_configure.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                  ctypes.c_double]
     lib.hr_get_ncyclebreak.restype = ctypes.c_long
     lib.hr_configure(lim, flux, 2, cour, 0, 1e30)
+    if limits is not None:
+        lib.hr_set_limits.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        lib.hr_set_limits(*[float(x) for x in limits])
     work = tempfile.mkdtemp(prefix="harmref_")
     devnull = os.open(os.devnull, os.O_WRONLY)
     saved = os.dup(2)
@@ -252,7 +256,7 @@ def _ref_worker(libpath, lim, flux, cour, nsteps, outpath, dump=False):
                          ncyclebreak=lib.hr_get_ncyclebreak(), **extra), f, protocol=4)
 
 
-def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800, dump=False):
+def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=1800, dump=False, limits=None):
     """Runs the compiled reference (init + nsteps steps) in a fresh child
     process (its init() can run once per process) and returns its arrays."""
     import pickle
@@ -262,8 +266,10 @@ def ref_run(n1, n2, lim=3, flux=1, cour=0.8, nsteps=1, problem="torus", timeout=
         return None
     fd, out = tempfile.mkstemp(suffix=".pkl", prefix="harmref_")
     os.close(fd)
-    code = ("import sys; sys.path.insert(0, %r); import harmtest; harmtest._ref_worker(%r, %d, %d, %r, %d, %r, %r)"
-            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, float(cour), nsteps, out, bool(dump)))
+    code = ("import sys; sys.path.insert(0, %r); import harmtest; "
+            "harmtest._ref_worker(%r, %d, %d, %r, %d, %r, %r, %r)"
+            % (os.path.dirname(os.path.abspath(__file__)), path, lim, flux, float(cour), nsteps, out, bool(dump),
+               None if limits is None else tuple(float(x) for x in limits)))
     try:
         r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
@@ -410,7 +416,7 @@ def ref_config(r):
     """harm config keyword arguments from a reference run's scalars."""
     s = r["scalars"]
     return dict(cour=s[12], gam=s[3], dx1=s[10], dx2=s[11], safe=s[20], defcon=s[21], gammamax=s[16],
-                gammafail=s[17], bsqorholimit=s[18], bsqoulimit=s[19])
+                gammafail=s[17], bsqorholimit=s[18], bsqoulimit=s[19], gammadamp=s[28], fluxadjust=int(s[29]))
 
 
 def interior(a):

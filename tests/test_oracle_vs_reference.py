@@ -70,3 +70,39 @@ def test_oracle_matches_reference_dipole_ffde(n1, n2, lim, flux, nsteps):
     # force-free state: no matter, field held fixed inside the star's surface
     assert not p[..., 0:2].any()
     assert np.array_equal(p[:3, 3:-3, 5:8], r["prims"][0][:3, 3:-3, 5:8])
+
+
+# the torus with the per-zone HLL/LAXF switch (FLUXADJUST FLUXBSQORHOANDU,
+# build "torusfa"): n, limiter, flux, steps, (BSQORHOLIMIT, BSQOULIMIT,
+# GAMMADAMP) or None for the reference's defaults.  With the defaults the
+# switch picks LAXF in a few zones only over these steps; the lowered
+# thresholds make it pick LAXF in 12-58% of the zones (and exercise the
+# check-solution votes of the b^2 flags much more)
+FLUXADJUST_LIMITS = (0.05, 0.02, 0.52)
+FLUXADJUST_CASES = [(32, 4, 1, 120, FLUXADJUST_LIMITS), (32, 3, 1, 100, FLUXADJUST_LIMITS), (32, 4, 1, 400, None)]
+
+
+@pytest.mark.parametrize("n,lim,flux,nsteps,limits", FLUXADJUST_CASES)
+def test_oracle_matches_reference_flux_switch(n, lim, flux, nsteps, limits):
+    r = ht.ref_run(n, n, lim=lim, flux=flux, nsteps=nsteps, problem="torusfa", limits=limits)
+    if r is None:
+        pytest.skip("reference build (oracle/_ref) with FLUXADJUST not present")
+    cfg = ht.ref_config(r)
+    assert cfg["fluxadjust"] == 3
+    if limits is not None:
+        assert (cfg["bsqorholimit"], cfg["bsqoulimit"], cfg["gammadamp"]) == limits
+    o = ht.Oracle(n, n, r["geom"], lim=lim, fluxmethod=flux, **cfg)
+    p = r["prims"][0].copy()
+    f = r["pflag"][0].copy()
+    t, dt = r["times"][0]
+    nlaxf = 0
+    for s in range(1, nsteps + 1):
+        rc, t, dt = o.step(p, f, t, dt)
+        assert rc == 0
+        assert np.array_equal(p, r["prims"][s]), f"step {s}: primitives differ"
+        # every flag, FLAGREALFLUX included, over the range get_bsqflags sets
+        assert np.array_equal(f[2:-2, 2:-2], r["pflag"][s][2:-2, 2:-2]), f"step {s}: flags differ"
+        assert (t, dt) == tuple(r["times"][s]), f"step {s}: t/dt differ"
+        nlaxf += int((f[2:-2, 2:-2, 4] == 0).sum())
+    assert nlaxf > 0, "the switch never picked LAXF"
+    print(f"\nflux switch, limits {limits}: {nlaxf} zone-steps with LAXF hydro fluxes")
