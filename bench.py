@@ -356,6 +356,10 @@ def b200_arm(a):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / a.e2e_steps, dist, "cuda")
     e2e = aggregate_rate(world, n * n, e2e_s)
 
+    # the device's FP64 instruction rate (own microbenchmark, CUDA events):
+    # the step's FP64 kernels run without multiply-add contraction, so their
+    # ceiling is the DADD/DMUL rate
+    fp64_rates = hb.measure_fp64_peak()
     # roofline of the dominant kernel (largest share of the step's device time)
     peak, peak_kind = peaks()
     dom = max(prof, key=lambda k: prof[k][0])
@@ -373,6 +377,19 @@ def b200_arm(a):
                 "whole_step": {"achieved": step_alg, "frac": step_alg / peak,
                                "bytes_per_zone_cycle": BYTES_PER_ZONE_CYCLE},
                 "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()}}
+    # the second ceiling: FP64 instructions the kernel issues per zone (ncu,
+    # FP64_INSTR_PER_ZONE) over its event-timed launch, against the measured
+    # DADD rate
+    fp64 = {"peak_dadd_per_s": fp64_rates["dadd"], "peak_dmul_per_s": fp64_rates["dmul"],
+            "peak_dfma_per_s": fp64_rates["dfma"], "how": "harm_measure_fp64_peak: independent DADD/DMUL/DFMA chains "
+                                                          "on every SM, CUDA events"}
+    for kname, per_zone in FP64_INSTR_PER_ZONE.items():
+        if kname in prof and prof[kname][1]:
+            ms_l = prof[kname][0] / prof[kname][1]
+            rate = per_zone * n * n / (ms_l * 1e-3)
+            fp64[kname] = {"fp64_instr_per_zone": per_zone, "achieved_per_s": rate, "launch_ms": ms_l,
+                           "frac_of_dadd_peak": rate / fp64_rates["dadd"]}
+    roofline["fp64"] = fp64
 
     mixed = None
     if not a.no_mixed:
@@ -772,6 +789,11 @@ KERNEL_BYTES = {
     "k_emf": 8 * (2 + 3 + 1),
     "k_bsqflags": 8 * (8 + 21) + 1,
 }
+# FP64 instructions (thread level, every FP64-pipe instruction: adds,
+# multiplies, the FMAs and comparisons of division and square root) per
+# active zone of one launch, from one ncu capture of each kernel at 512^2
+# (sm__inst_executed_pipe_fp64.sum x 32 / zones; profiles/)
+FP64_INSTR_PER_ZONE = {}
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
 # at 512^2 (profiles/k_*_torus512_fp64_para_hll.md), scaled by zone count
 TRAFFIC_512 = {"k_flux": 113.8e6, "k_update": 212.2e6}

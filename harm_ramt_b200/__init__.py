@@ -105,20 +105,18 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
 
 
 def load_library(path=None):
-    """Loads libharm_b200.so (building it first when nvcc is available and
-    the sources are newer).  Raises if the library cannot be loaded."""
+    """Loads libharm_b200.so, building it first when its sources are newer
+    (a failed build raises: a library older than its sources is never used
+    silently).  With HARM_PREBUILT_ONLY=1 in the environment the library in
+    the package is loaded as it is.  Raises if it cannot be loaded."""
     global _lib
     if _lib is not None and path is None:
         return _lib
     p = path or LIB_PATH
-    if path is None:
-        try:
-            from . import build as _build
-            if _build.needs_build():
-                _build.build()
-        except Exception as e:  # a prebuilt library is still usable
-            if not os.path.exists(p):
-                raise RuntimeError(f"libharm_b200.so is missing and could not be built: {e}") from e
+    if path is None and not os.environ.get("HARM_PREBUILT_ONLY"):
+        from . import build as _build
+        if _build.needs_build():
+            _build.build()
     lib = ctypes.CDLL(p)
     vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
     lib.harm_create.argtypes = [ctypes.POINTER(_Config), vp, ctypes.POINTER(vp)]

@@ -20,6 +20,8 @@
 
 #include "../../include/harm_b200.h"
 #include "harm_kernels.cuh"
+#include "harm_tma.cuh"
+#include <cudaTypedefs.h>
 
 namespace harm {
 __global__ void k_bsqflags(StepArgs a, const double* pv);
@@ -84,7 +86,9 @@ struct harm_ctx {
   cudaGraph_t graph;
   cudaGraphExec_t gexec;
   bool have_graph;
-  dim3 tile_update;  // k_update block (at most 128 threads)
+  dim3 tile_update;  // k_update block (at most 128 threads, even width)
+  CUtensorMap geo_map;  // k_update's TMA box over the geometry block (tile_update + 2 columns)
+  CUtensorMap map_p, map_pk0;  // k_flux's TMA boxes over the state p and the midpoint state pk[0]
   dim3 tile_small;   // block of the stencil/fixup/boundary kernels
   StepArgs args() const
   {
@@ -145,6 +149,45 @@ struct harm_ctx {
   } while (0)
 
 static dim3 grid2(int ni, int nj, dim3 b) { return dim3((ni + b.x - 1) / b.x, (nj + b.y - 1) / b.y); }
+
+namespace harm {
+bool tma_encode_planes(CUtensorMap* map, const double* base, int pitch, int rows, int nplanes, long long plane, int bx,
+                       int by, int bz)
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+  if (!enc) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)rows, (cuuint64_t)nplanes};
+  const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)plane * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace harm
+
+// k_flux's map over a state's 8 planes, the box of one block's tile
+static bool encode_prim_map(CUtensorMap* map, const double* prims, const Grid& gr, int flux_by)
+{
+  if ((uintptr_t)prims & 15) return false;
+  return tma_encode_planes(map, prims, gr.pitch, gr.rows, NPR, gr.plane, FLUX_TILE_W, flux_tile_rows(flux_by), NPR);
+}
+
+// k_update's map: the geometry block, boxes of the block's zones (and one
+// column more on each side) over the 42 connection and floor planes
+static bool encode_geo_map(CUtensorMap* map, const double* geo, const Grid& gr, dim3 ub)
+{
+  if ((ub.x & 1) || ((uintptr_t)geo & 15)) return false;
+  return tma_encode_planes(map, geo, gr.pitch, gr.rows, GEO_NPLANES, gr.plane, (int)upd_box_w(ub.x), (int)ub.y,
+                           UPD_STAGED);
+}
 
 // kernel classes of one step, in launch order (for per-kernel timing)
 enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_CHECKSOL, KC_CHECKSERIAL, KC_FIXC,
@@ -226,11 +269,12 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     const int mixed = c->cfg.precision == HARM_PREC_MIXED;
     const int ffde = c->cfg.eom == HARM_EOM_FFDE;
     const bool poledeath = c->cfg.bc == HARM_BC_TORUS;
-    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2, c->flux_by), fb, s, a, pb);
+    launch_flux(c->cfg.lim == HARM_LIM_PARA, mixed, ffde, flux_grid(n1, n2, c->flux_by), fb, s, a,
+                (sub == 0) ? c->map_p : c->map_pk0);
     T.mark(s, KC_FLUX);
     launch_emf(mixed, grid2(n1 + 2, n2 + 2, b), b, s, a, c->d_p);
     T.mark(s, KC_EMF);
-    launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, pi, pb, pf, c2);
+    launch_update(mixed, ffde, grid2(n1, n2, ub), ub, s, a, c->geo_map, pi, pb, pf, c2);
     T.mark(s, KC_UPDATE, ffde ? 1 : 2);  // k_update and k_update_tail
     if (rec) {
       cudaMemcpyAsync(rec->upd[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
@@ -367,6 +411,12 @@ int harm_create(const harm_config* cfg, void* stream, harm_ctx** out)
   if (!ok) {
     harm_destroy(c);
     return HARM_ENOMEM;
+  }
+  if (!encode_geo_map(&c->geo_map, c->d_geo, c->gr, c->tile_update) ||
+      !encode_prim_map(&c->map_p, c->d_p, c->gr, c->flux_by) || !encode_prim_map(&c->map_pk0, c->d_pk0, c->gr, c->flux_by)) {
+    fprintf(stderr, "harm_b200: a TMA map (geometry or state planes) could not be encoded\n");
+    harm_destroy(c);
+    return HARM_ECUDA;
   }
   cudaMemsetAsync(c->d_p, 0, NPR * pd, c->stream);
   cudaMemsetAsync(c->d_pk0, 0, NPR * pd, c->stream);
@@ -770,9 +820,13 @@ int harm_set_tiles(harm_ctx* c, const harm_tiles* t)
 {
   if (!c || !t) return HARM_EINVAL;
   const long long nu = (long long)t->update_x * t->update_y, ns = (long long)t->small_x * t->small_y;
-  if (t->update_x < 1 || t->update_y < 1 || nu > 128 || t->small_x < 1 || t->small_y < 1 || ns > 1024)
+  if (t->update_x < 2 || (t->update_x & 1) || t->update_y < 1 || nu > 128 || t->small_x < 1 || t->small_y < 1 ||
+      ns > 1024)
     return HARM_EINVAL;
   CK(cudaStreamSynchronize(c->stream));
+  CUtensorMap m;
+  if (!encode_geo_map(&m, c->d_geo, c->gr, dim3(t->update_x, t->update_y))) return HARM_ECUDA;
+  c->geo_map = m;
   c->tile_update = dim3(t->update_x, t->update_y);
   c->tile_small = dim3(t->small_x, t->small_y);
   drop_graph(c);
@@ -1444,6 +1498,11 @@ extern "C" int harm_step_noalloc(const harm_config* cfg, const double* d_geo, do
   c.d_bsqf = (unsigned char*)(s + NA_OFF_BYTES);
   c.d_chk = c.d_bsqf + pl;
   c.d_fluxf = cfg->fluxadjust ? c.d_chk + 2 * pl : nullptr;
+  if (!encode_geo_map(&c.geo_map, d_geo, c.gr, c.tile_update) || !encode_prim_map(&c.map_p, d_prims, c.gr, c.flux_by) ||
+      !encode_prim_map(&c.map_pk0, c.d_pk0, c.gr, c.flux_by)) {
+    fprintf(stderr, "harm_step_noalloc: d_geo and d_prims must be 16-byte aligned (their TMA maps could not be encoded)\n");
+    return HARM_EINVAL;
+  }
   c.geo_ok = true;
   // the array keeps the last call's contents: the run scalars start from
   // zero on every call, the check-solution gamma table only when asked

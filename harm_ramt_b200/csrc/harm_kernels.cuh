@@ -9,6 +9,7 @@
 //   gcon + 1 gdet planes; 40 connection planes Gamma^k_{(lj)} at CENT; 2 floor
 //   planes.  Fluxes: 8 planes per direction.
 #pragma once
+#include <cuda.h>
 #include "harm_device.cuh"
 
 namespace harm {
@@ -30,6 +31,15 @@ constexpr int GEO_FLOOR = GEO_CONN + 40;        // 2 floor planes
 constexpr int GEO_NPLANES = GEO_FLOOR + 2;
 
 __host__ __device__ constexpr int conn_plane(int k, int l, int j) { return GEO_CONN + k * 10 + sym(l, j); }
+
+// k_update's staged geometry: the 40 connection planes and the 2 floor
+// planes (GEO_CONN .. GEO_NPLANES-1, contiguous) of the block's zones, one
+// TMA box of (block width + 2) columns x block height rows x 42 planes.  The
+// box starts on the even column at or before the block's first zone (the
+// block width is even), so the zone of thread (tx, ty) sits at column tx + 1.
+constexpr int UPD_STAGED = GEO_NPLANES - GEO_CONN;
+__host__ __device__ constexpr int upd_box_w(int bx) { return bx + 2; }
+__host__ __device__ inline size_t upd_smem_bytes(int bx, int by) { return (size_t)UPD_STAGED * by * upd_box_w(bx) * sizeof(double); }
 
 struct Params {
   int lim;          // 3 MC, 4 PARA
@@ -171,6 +181,20 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 // of the mixed form fit 128 registers without spilling and run best as
 // 4-row blocks at four per SM on any grid.
 constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = 16;
+// k_flux's primitive tile (one TMA box over a state's 8 planes): the 32
+// columns of the block's zones and 2 more on each side (PARA's stencil) = 36,
+// starting on the even column at or before the first (TMA copies start on
+// 16-byte boundaries) = 37, rounded to 38 (a row of the box is a multiple of
+// 16 bytes); BY rows, 2 more on each side, and one more below for the x2
+// neighbour of the first row.  The box's first row is the zone row of the
+// block's first zones minus 3 (row -1 of the plane for the first blocks,
+// which reads as zero and is never used).
+constexpr int FLUX_TILE_W = 38;
+__host__ __device__ constexpr int flux_tile_rows(int by) { return by + 5; }
+__host__ __device__ constexpr size_t flux_tile_bytes(int by)
+{
+  return (size_t)NPR * flux_tile_rows(by) * FLUX_TILE_W * sizeof(double);
+}
 inline dim3 flux_grid(int n1, int n2, int by) { return dim3((n1 + 1 + FLUX_BX - 1) / FLUX_BX, (n2 + 2 + by - 1) / by); }
 inline int flux_rows(int n1, int n2, bool fp32_faces)
 {
@@ -184,14 +208,16 @@ constexpr int CUR_RING = 0, CUR_S1 = 9, CUR_S2 = 12, CUR_FCON = 15, CUR_JCON = 2
 
 // launchers of the templated step kernels (harm_step.cu: FP64 instantiations
 // and dispatch; harm_step_mixed.cu: the mixed-precision instantiations)
-void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a,
+                 const CUtensorMap& prim_map);
 void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv);
-void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
-                   const double* pb, double* pf, double c2);
+void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map,
+                   const double* pi, const double* pb, double* pf, double c2);
 void launch_step_end(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
-void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb);
+void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a,
+                       const CUtensorMap& prim_map);
 void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv);
-void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
-                         const double* pb, double* pf, double c2);
+void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map,
+                         const double* pi, const double* pb, double* pf, double c2);
 
 }  // namespace harm

@@ -81,7 +81,8 @@ __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __
       for (int k = 0; k < NPR; k++) pr0[k] = pi[k * pl + z];
       pfl = ta::tryagain_chain(U, g, a.pp.gam, a.pp.gammafail, pr0, pfz, pfl);
     }
-    finish_zone(a, g, z, i, j, pfz, pfl, pf);
+    finish_zone(a, g, z, i, j, pfz, pfl, pf, __ldg(a.geo + (long long)GEO_FLOOR * pl + z),
+                __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z));
     atomicAdd(&a.sc->newton_iters, (unsigned long long)niter);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.sc->ndeferred_total += nd;
@@ -798,14 +799,15 @@ __global__ void k_planes_to_ref(StepArgs a, const double* __restrict__ pv, doubl
 // launchers of the templated kernels: the FP64 instantiations here, the
 // mixed-precision ones in harm_step_mixed.cu
 
-void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+void launch_flux(int para, int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a,
+                 const CUtensorMap& prim_map)
 {
-  if (mixed) launch_flux_mixed(para, ffde, g, b, s, a, pb);
+  if (mixed) launch_flux_mixed(para, ffde, g, b, s, a, prim_map);
   else if (ffde) {
-    if (para) flux_rows_launch<double, true, true>(g, b, s, a, pb);
-    else flux_rows_launch<double, false, true>(g, b, s, a, pb);
-  } else if (para) flux_rows_launch<double, true, false>(g, b, s, a, pb);
-  else flux_rows_launch<double, false, false>(g, b, s, a, pb);
+    if (para) flux_rows_launch<double, true, true>(g, b, s, a, prim_map);
+    else flux_rows_launch<double, false, true>(g, b, s, a, prim_map);
+  } else if (para) flux_rows_launch<double, true, false>(g, b, s, a, prim_map);
+  else flux_rows_launch<double, false, false>(g, b, s, a, prim_map);
 }
 
 void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv)
@@ -814,12 +816,12 @@ void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, co
   else k_emf<double><<<g, b, 0, s>>>(a, pv);
 }
 
-void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
-                   const double* pb, double* pf, double c2)
+void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map,
+                   const double* pi, const double* pb, double* pf, double c2)
 {
-  if (mixed) launch_update_mixed(ffde, g, b, s, a, pi, pb, pf, c2);
-  else if (ffde) k_update<double, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
-  else k_update<double, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  if (mixed) launch_update_mixed(ffde, g, b, s, a, map, pi, pb, pf, c2);
+  else if (ffde) update_launch<double, true>(g, b, s, a, map, pi, pb, pf, c2);
+  else update_launch<double, false>(g, b, s, a, map, pi, pb, pf, c2);
   if (!ffde) {
     if (a.pp.tryagain) k_update_tail<true><<<148, 64, 0, s>>>(a, pi, pf);
     else k_update_tail<false><<<148, 64, 0, s>>>(a, pi, pf);

@@ -5,30 +5,31 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "harm_kernels.cuh"
+#include "harm_tma.cuh"
 
 namespace harm {
 
 // ---------------------------------------------------------------- fluxes
-// Interface states of zone (i, j) along `dir` (step_ch.c:812-823 slopes and
-// 893-904 interface values): L = the zone's left-face value (p_r of face i),
-// R = its right-face value (p_l of face i+1).
+// Interface states of a zone along `dir` (step_ch.c:812-823 slopes and
+// 893-904 interface values) from its stencil in the block's primitive tile
+// (shared memory): L = the zone's left-face value (p_r of face i), R = its
+// right-face value (p_l of face i+1).  t points at the zone's value of
+// plane 0; planes are `ps` doubles apart, the stencil step is `st` (1 along
+// x1, the tile width along x2).
 template <typename T, bool PARA>
-__device__ __forceinline__ void zone_states(const StepArgs& a, const double* __restrict__ pb, int i, int j, int dir,
-                                            T* L, T* R)
+__device__ __forceinline__ void zone_states(const double* t, int ps, int st, T* L, T* R)
 {
-  const long long s = (dir == 1) ? 1LL : (long long)a.gr.pitch;
-  const long long z = a.gr.at(i, j);
 #pragma unroll
   for (int k = 0; k < NPR; k++) {
-    const double* pk = pb + k * a.gr.plane + z;
+    const double* pk = t + k * ps;
     if (!PARA) {
-      T ym1 = (T)__ldg(pk - s), y0 = (T)__ldg(pk), yp1 = (T)__ldg(pk + s);
+      T ym1 = (T)pk[-st], y0 = (T)pk[0], yp1 = (T)pk[st];
       T dq = mc_slope(ym1, y0, yp1);
       L[k] = y0 - T(0.5) * dq;
       R[k] = y0 + T(0.5) * dq;
     } else {
       T l, r;
-      para4((T)__ldg(pk - 2 * s), (T)__ldg(pk - s), (T)__ldg(pk), (T)__ldg(pk + s), (T)__ldg(pk + 2 * s), l, r);
+      para4((T)pk[-2 * st], (T)pk[-st], (T)pk[0], (T)pk[st], (T)pk[2 * st], l, r);
       L[k] = l;
       R[k] = r;
     }
@@ -36,7 +37,11 @@ __device__ __forceinline__ void zone_states(const StepArgs& a, const double* __r
 }
 
 // Flux through one face from its two interface states (the rest of the
-// fluxcalc face loop, step_ch.c:944-1065).
+// fluxcalc face loop, step_ch.c:944-1065).  The left state is finished
+// (state, fluxes, wavespeeds) before the right one starts, and U_r - U_l is
+// formed as soon as U_r exists, so only one state is live at a time; the
+// values and the order of the fatal checks (both Lorentz limits, then the
+// left and the right wavespeeds) are the reference's.
 template <typename T, bool FFDE>
 __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int dir, T* p_l, T* p_r, T* Fo,
                                           double& dtij)
@@ -51,17 +56,25 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   const T gmax = (T)a.pp.gammamax, gam = (T)a.pp.gam;
   int rc = limit_gamma(gmax, p_l, g);
   if (!rc) rc = limit_gamma(gmax, p_r, g);
-  State<T> ql, qr;
-  state_of(p_l, g, ql);
-  state_of(p_r, g, qr);
-  T F_l[NPR], F_r[NPR], U_l[NPR], U_r[NPR];
-  flux_of<T, FFDE>(p_l, ql, dir, g, gam, F_l);
-  flux_of<T, FFDE>(p_r, qr, dir, g, gam, F_r);
-  flux_of<T, FFDE>(p_l, ql, 0, g, gam, U_l);
-  flux_of<T, FFDE>(p_r, qr, 0, g, gam, U_r);
+  T F_l[NPR], F_r[NPR], dU[NPR];
   T cmax_l, cmin_l, cmax_r, cmin_r;
-  if (!rc) rc = vchar_of(p_l, ql, dir, g, gam, cmax_l, cmin_l);
-  if (!rc) rc = vchar_of(p_r, qr, dir, g, gam, cmax_r, cmin_r);
+  {
+    State<T> q;
+    state_of(p_l, g, q);
+    flux_of<T, FFDE>(p_l, q, dir, g, gam, F_l);
+    flux_of<T, FFDE>(p_l, q, 0, g, gam, dU);  // U_l for now
+    if (!rc) rc = vchar_of(p_l, q, dir, g, gam, cmax_l, cmin_l);
+  }
+  {
+    State<T> q;
+    T U_r[NPR];
+    state_of(p_r, g, q);
+    flux_of<T, FFDE>(p_r, q, dir, g, gam, F_r);
+    flux_of<T, FFDE>(p_r, q, 0, g, gam, U_r);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) dU[k] = U_r[k] - dU[k];
+    if (!rc) rc = vchar_of(p_r, q, dir, g, gam, cmax_r, cmin_r);
+  }
   if (rc) {
     report_fail(a.sc, a.phase0 + (dir == 1 ? PH_FACE1 : PH_FACE2), rc, zone_order(i, j));
     cmax_l = cmin_l = cmax_r = cmin_r = T(0.);
@@ -75,18 +88,17 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   // (HYDROFLUXADJUSTONLY 1) the hydro variables follow FLAGREALFLUX of zone
   // (i, j), the face's own zone
   const int rf = a.pp.fluxadjust ? (int)a.fluxf[z] : a.pp.fluxmethod;
-  const T hll_h = (rf == 1) ? T(1.0) : T(0.0), laxf_h = (rf == 1) ? T(0.0) : T(1.0);
-  const T hll_b = (a.pp.fluxmethod == 1) ? T(1.0) : T(0.0), laxf_b = (a.pp.fluxmethod == 1) ? T(0.0) : T(1.0);
   if (cmax + cmin != T(0.0)) {
 #pragma unroll
     for (int k = 0; k < NPR; k++) {
-      const T hllfrac = (k < B1) ? hll_h : hll_b, laxffrac = (k < B1) ? laxf_h : laxf_b;
-      Fo[k] = hllfrac * ((cmax * F_l[k] + cmin * F_r[k] - cmax * cmin * (U_r[k] - U_l[k])) / (cmax + cmin)) +
-              laxffrac * (T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k])));
+      const int m = (k < B1) ? rf : a.pp.fluxmethod;
+      const T hllfrac = (m == 1) ? T(1.0) : T(0.0), laxffrac = (m == 1) ? T(0.0) : T(1.0);
+      Fo[k] = hllfrac * ((cmax * F_l[k] + cmin * F_r[k] - cmax * cmin * dU[k]) / (cmax + cmin)) +
+              laxffrac * (T(0.5) * (F_l[k] + F_r[k] - ctop * dU[k]));
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < NPR; k++) Fo[k] = T(0.5) * (F_l[k] + F_r[k] - ctop * (U_r[k] - U_l[k]));
+    for (int k = 0; k < NPR; k++) Fo[k] = T(0.5) * (F_l[k] + F_r[k] - ctop * dU[k]);
   }
   // face Courant limit, step_ch.c:1062-1065 (kept in FP64)
   double cm = (double)rmax(cmax, cmin);
@@ -118,37 +130,56 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // with i >= 0, x2 faces with j >= 0 (FZLOOP ranges), then the fix_flux
 // rules that do not read another face (fixup.c:1357-1410; the inner x1 mass
 // flux clamp only where that end is OUTFLOW, i.e. for the torus).  Blocks are
-// 32 (x1) x FLUX_BY (x2) zones; every zone reconstructs its own interface
-// states once: the x1 neighbour's right state arrives by warp shuffle and
-// the x2 neighbour's through shared memory (the first row recomputes).
-// Lane 0's zone is also the previous block's lane 31 (blocks step by
-// FLUX_BX = 31 along x1): lane 0 only lends its right state, and its faces
-// are the previous block's (block 0's lane 0 is zone -1, which has no x1
-// face but an x2 face).
+// 32 (x1) x BY (x2) zones.  The block's primitive tile -- its zones, the
+// two-zone stencil halo on every side and one more row below, for the x2
+// neighbour of its first row -- arrives in shared memory by one TMA copy
+// (flux_tile_*, below); every zone reconstructs its own interface states
+// once from the tile: the x1 neighbour's right state arrives by warp
+// shuffle and the x2 neighbour's through shared memory (the first row
+// recomputes it).  Lane 0's zone is also the previous block's lane 31
+// (blocks step by FLUX_BX = 31 along x1): lane 0 only lends its right state,
+// and its faces are the previous block's (block 0's lane 0 is zone -1,
+// which has no x1 face but an x2 face).
 // BY = 4 or 16 rows per block (flux_rows).  At most 128 registers a thread:
 // 512 threads per SM for the FP64 faces, four 4-row blocks for the FP32 ones.
 template <typename T, bool PARA, bool FFDE, int BY>
-__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 4 : 1)) k_flux(StepArgs a, const double* __restrict__ pb)
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 4 : 1))
+    k_flux(StepArgs a, const __grid_constant__ CUtensorMap prim_map)
 {
+  extern __shared__ __align__(128) double tile[];
   __shared__ double sh[2][32];
   __shared__ T shr[NPR][BY][32];
+  __shared__ uint64_t bar;
   const int tx = threadIdx.x, ty = threadIdx.y;
+  constexpr int ROWS = flux_tile_rows(BY), PS = ROWS * FLUX_TILE_W;
+  const int cx = (int)(blockIdx.x * FLUX_BX) & ~1;  // the tile's first column (even)
+  if (tx == 0 && ty == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, (uint32_t)flux_tile_bytes(BY));
+    tma_load_3d(tile, &prim_map, cx, (int)(blockIdx.y * BY) - 1, 0, &bar);
+  }
   const int i = blockIdx.x * FLUX_BX + tx - 1;
   const int j = blockIdx.y * BY + ty - 1;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   const bool in = (i <= n1) && (j <= n2);
   const bool own = (tx > 0) || (blockIdx.x == 0);  // lane 0 of a later block repeats a zone
-  // threads past the grid work on a clamped (valid) zone; their results are unused
-  const int ic = (i <= n1) ? i : n1, jc = (j <= n2) ? j : n2;
+  const long long z = a.gr.at(in ? i : -1, in ? j : -1);
   double dt1 = 1.e9, dt2 = 1.e9;
-  const long long z = a.gr.at(ic, jc);
   T L[NPR], R[NPR], pl[NPR];
   T Fo[NPR];
   double dtij;
   T* F1 = reinterpret_cast<T*>(a.F1);
   T* F2 = reinterpret_cast<T*>(a.F2);
+  __syncthreads();  // the barrier is initialised before anyone polls it
+  if (!mbar_wait(&bar, 0)) {
+    if (tx == 0 && ty == 0) report_fail(a.sc, a.phase0 + PH_FACE1, FAIL_TMA_TIMEOUT, zone_order(i, j));
+    return;
+  }
+  // the zone's value of plane 0 in the tile: row ty + 3, column tx + 2 + (the
+  // block's first column - cx)
+  const double* tz = tile + (ty + 3) * FLUX_TILE_W + tx + 2 + ((int)(blockIdx.x * FLUX_BX) - cx);
   // ---- x1 faces
-  zone_states<T, PARA>(a, pb, ic, jc, 1, L, R);
+  zone_states<T, PARA>(tz, PS, 1, L, R);
 #pragma unroll
   for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
   if (in && i >= 0 && tx > 0) {
@@ -160,16 +191,16 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
     for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
   }
   // ---- x2 faces
-  zone_states<T, PARA>(a, pb, ic, jc, 2, L, R);
+  zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
 #pragma unroll
   for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
   __syncthreads();
   if (ty > 0) {
 #pragma unroll
     for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
-  } else if (jc >= 0) {
+  } else {
     T Lm[NPR];
-    zone_states<T, PARA>(a, pb, ic, jc - 1, 2, Lm, pl);
+    zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
   }
   if (in && j >= 0 && own) {
     face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
@@ -193,12 +224,24 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
   }
 }
 
-// the k_flux instance of the block's row count (b.y)
-template <typename T, bool PARA, bool FFDE>
-inline void flux_rows_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+// the k_flux instance of the block's row count (b.y); its dynamic shared
+// memory limit raised once to the tile's size
+template <typename T, bool PARA, bool FFDE, int BY>
+inline void flux_launch_by(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map)
 {
-  if (b.y == FLUX_BY_LARGE) k_flux<T, PARA, FFDE, FLUX_BY_LARGE><<<g, b, 0, s>>>(a, pb);
-  else k_flux<T, PARA, FFDE, FLUX_BY_SMALL><<<g, b, 0, s>>>(a, pb);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_flux<T, PARA, FFDE, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_tile_bytes(BY));
+    attr = true;
+  }
+  k_flux<T, PARA, FFDE, BY><<<g, b, flux_tile_bytes(BY), s>>>(a, map);
+}
+template <typename T, bool PARA, bool FFDE>
+inline void flux_rows_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map)
+{
+  if (b.y == FLUX_BY_LARGE) flux_launch_by<T, PARA, FFDE, FLUX_BY_LARGE>(g, b, s, a, map);
+  else flux_launch_by<T, PARA, FFDE, FLUX_BY_SMALL>(g, b, s, a, map);
 }
 
 // flux_ct corner EMF, step_ch.c:1214-1234, over i in [0,N1], j in [0,N2].
@@ -248,9 +291,9 @@ __global__ void k_emf(StepArgs a, const double* __restrict__ pv)
 constexpr int NEWTON_MAIN_CAP = 16;
 
 // pflag store + fixup1zone (fixup.c:274-377: floors then the Lorentz factor
-// limit) + store of the new primitives
+// limit) + store of the new primitives; frho, fu: the zone's floors
 __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>& g, long long z, int i, int j, double* pfz,
-                                            int pfl, double* pf)
+                                            int pfl, double* pf, double frho, double fu)
 {
   const long long pl = a.gr.plane;
   if (a.rec_pinv) {
@@ -258,7 +301,6 @@ __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>
     for (int k = 0; k < NPR; k++) a.rec_pinv[k * pl + z] = pfz[k];
   }
   a.pflag[z] = pfl;
-  const double frho = __ldg(a.geo + (long long)GEO_FLOOR * pl + z), fu = __ldg(a.geo + (long long)(GEO_FLOOR + 1) * pl + z);
   if (frho > pfz[RHO]) pfz[RHO] = frho;
   if (fu > pfz[UU]) pfz[UU] = fu;
   int rc = limit_gamma(a.pp.gammamax, pfz, g);
@@ -269,33 +311,85 @@ __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>
 
 // advance_standard zone loop, advance.c:114-181, for one RK2 substep.
 // CUf = {1, 0, c2}: Uf = Ui + c2*dt*dU; on the last substep unew = Uf.
+// The connection coefficients and floors arrive by TMA (geo_map, a 3D map
+// over the geometry block with the box above) while U(p_i) and the flux
+// divergence are formed from global loads; the block width is even.
 template <typename FT, bool FFDE>
-__global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __restrict__ pi, const double* __restrict__ pb,
+__global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const __grid_constant__ CUtensorMap geo_map,
+                                                const double* __restrict__ pi, const double* __restrict__ pb,
                                                 double* __restrict__ pf, double c2)
 {
+  extern __shared__ __align__(128) double sgeo[];
+  __shared__ uint64_t bar;
   const FT* F1 = reinterpret_cast<const FT*>(a.F1);
   const FT* F2 = reinterpret_cast<const FT*>(a.F2);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= a.gr.n1 || j >= a.gr.n2) return;
-  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  const int W = upd_box_w(blockDim.x);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, (uint32_t)upd_smem_bytes(blockDim.x, blockDim.y));
+    tma_load_3d(sgeo, &geo_map, (int)((blockIdx.x * blockDim.x + NG) & ~1u), (int)(blockIdx.y * blockDim.y + NG),
+                GEO_CONN, &bar);
+  }
+  __syncthreads();  // the barrier is initialised before anyone polls it
+  const bool active = (i < a.gr.n1 && j < a.gr.n2);
+  const long long pl = a.gr.plane, z = a.gr.at(active ? i : 0, active ? j : 0);
   const double dt = a.sc->dt;
   Geo<double> g;
-  load_geo(a, CENT, z, g);
   const double gam = a.pp.gam;
-  double U[NPR], pfz[NPR];
-  {
-    // Ui = U(pi)
-    double pr[NPR];
+  double U[NPR], pfz[NPR], dUr[NPR];
+  if (active) {
+    load_geo(a, CENT, z, g);
+    {
+      // Ui = U(pi)
+      double pr[NPR];
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pr[k] = __ldg(pi + k * pl + z);
+      for (int k = 0; k < NPR; k++) pr[k] = __ldg(pi + k * pl + z);
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pfz[k] = pr[k];
-    State<double> q;
-    state_of(pr, g, q);
-    flux_of<double, FFDE>(pr, q, 0, g, gam, U);
-    if (a.bsqf_fused) a.bsqf_fused[z] = bsq_flag(a, pr, q);  // get_bsqflags of the step's p
+      for (int k = 0; k < NPR; k++) pfz[k] = pr[k];
+      State<double> q;
+      state_of(pr, g, q);
+      flux_of<double, FFDE>(pr, q, 0, g, gam, U);
+      if (a.bsqf_fused) a.bsqf_fused[z] = bsq_flag(a, pr, q);  // get_bsqflags of the step's p
+    }
+    {
+      // flux divergence with flux-CT B fluxes (step_ch.c:1403-1413)
+      const double idx1 = 1.0 / a.pp.dx1, idx2 = 1.0 / a.pp.dx2;
+      const long long zi1 = a.gr.at(i + 1, j), zj1 = a.gr.at(i, j + 1), zij = a.gr.at(i + 1, j + 1);
+      const double e00 = a.emf[z], e10 = a.emf[zi1], e01 = a.emf[zj1], e11 = a.emf[zij];
+#pragma unroll
+      for (int k = 0; k < NPR; k++) {
+        double f1p, f1m, f2p, f2m;
+        if (k == B1) {
+          f1p = 0.;
+          f1m = 0.;
+          f2m = -0.5 * (e00 + e10);
+          f2p = -0.5 * (e01 + e11);
+        } else if (k == B2) {
+          f1m = 0.5 * (e00 + e01);
+          f1p = 0.5 * (e10 + e11);
+          f2p = 0.;
+          f2m = 0.;
+        } else {
+          f1p = F1[k * pl + zi1];
+          f1m = F1[k * pl + z];
+          f2p = F2[k * pl + zj1];
+          f2m = F2[k * pl + z];
+        }
+        const double dU1 = (-(f1p - f1m) * idx1);
+        const double dU2 = (-(f2p - f2m) * idx2);
+        dUr[k] = dU1 + dU2;
+      }
+    }
   }
+  if (!mbar_wait(&bar, 0)) {
+    if (active) report_fail(a.sc, a.phase0 + PH_UPDATE, FAIL_TMA_TIMEOUT, zone_order(i, j));
+    return;
+  }
+  if (!active) return;
+  const int plane_s = blockDim.y * W;
+  const double* sz = sgeo + threadIdx.y * W + threadIdx.x + 1;
   double dUg[NPR];
   {
     // source_conn, phys.c:520-619: dU[UU+l] = e * sum_j sum_k T^j_k Gamma^k_{lj}
@@ -305,7 +399,6 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
     State<double> q;
     state_of(pr, g, q);
     double acc[4] = {0., 0., 0., 0.};
-    const double* cn = a.geo + z;
 #pragma unroll
     for (int jj = 0; jj < 4; jj++) {
       double row[4];
@@ -313,7 +406,7 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
 #pragma unroll
       for (int l = 0; l < 4; l++)
 #pragma unroll
-        for (int k = 0; k < 4; k++) acc[l] += row[k] * __ldg(cn + (long long)conn_plane(k, l, jj) * pl);
+        for (int k = 0; k < 4; k++) acc[l] += row[k] * sz[(conn_plane(k, l, jj) - GEO_CONN) * plane_s];
     }
     dUg[RHO] = 0. + g.g * 0.;
     dUg[B1] = dUg[B2] = dUg[B3] = dUg[RHO];
@@ -321,36 +414,10 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
     for (int l = 0; l < 4; l++) dUg[UU + l] = 0. + g.g * acc[l];
   }
   {
-    // flux divergence with flux-CT B fluxes (step_ch.c:1403-1413) and the
-    // RK combine of dUtoU, advance.c:273-286
-    const double idx1 = 1.0 / a.pp.dx1, idx2 = 1.0 / a.pp.dx2;
-    const long long zi1 = a.gr.at(i + 1, j), zj1 = a.gr.at(i, j + 1), zij = a.gr.at(i + 1, j + 1);
-    const double e00 = a.emf[z], e10 = a.emf[zi1], e01 = a.emf[zj1], e11 = a.emf[zij];
+    // the RK combine of dUtoU, advance.c:273-286
     const double cdt = c2 * dt;
 #pragma unroll
-    for (int k = 0; k < NPR; k++) {
-      double f1p, f1m, f2p, f2m;
-      if (k == B1) {
-        f1p = 0.;
-        f1m = 0.;
-        f2m = -0.5 * (e00 + e10);
-        f2p = -0.5 * (e01 + e11);
-      } else if (k == B2) {
-        f1m = 0.5 * (e00 + e01);
-        f1p = 0.5 * (e10 + e11);
-        f2p = 0.;
-        f2m = 0.;
-      } else {
-        f1p = F1[k * pl + zi1];
-        f1m = F1[k * pl + z];
-        f2p = F2[k * pl + zj1];
-        f2m = F2[k * pl + z];
-      }
-      const double dU1 = (-(f1p - f1m) * idx1);
-      const double dU2 = (-(f2p - f2m) * idx2);
-      const double dUr = dU1 + dU2;
-      U[k] = 1.0 * U[k] + 0.0 * 0.0 + cdt * (dUr + dUg[k]);
-    }
+    for (int k = 0; k < NPR; k++) U[k] = 1.0 * U[k] + 0.0 * 0.0 + cdt * (dUr[k] + dUg[k]);
   }
   if constexpr (FFDE) {
     // Utoprim_ffde, then fixup1zone's Lorentz-factor limit (the floors are
@@ -373,7 +440,8 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
     a.worklist[atomicAdd(&a.sc->ndeferred, 1)] = (int)z;
     niter = 0;
   } else {
-    finish_zone(a, g, z, i, j, pfz, pfl, pf);
+    finish_zone(a, g, z, i, j, pfz, pfl, pf, sz[(GEO_FLOOR - GEO_CONN) * plane_s],
+                sz[(GEO_FLOOR + 1 - GEO_CONN) * plane_s]);
   }
   // Newton iteration count (the reference's nstroke), one atomic per warp
   const unsigned mask = __activemask();
@@ -382,6 +450,27 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const double* __r
 }
 
 
+
+// launches a k_update instance (its dynamic shared memory limit raised once
+// to the largest box of the tile shapes harm_set_tiles accepts: 42 planes x
+// at most 128 threads)
+template <typename FT, bool FFDE>
+inline void update_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map, const double* pi,
+                          const double* pb, double* pf, double c2)
+{
+  static bool attr = false;
+  if (!attr) {
+    size_t mx = 0;
+    for (int by = 1; by <= 128; by++) {
+      const int bx = 128 / by;
+      const size_t v = upd_smem_bytes(bx + (bx & 1), by);
+      if (v > mx) mx = v;
+    }
+    cudaFuncSetAttribute(k_update<FT, FFDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+    attr = true;
+  }
+  k_update<FT, FFDE><<<g, b, upd_smem_bytes(b.x, b.y), s>>>(a, map, pi, pb, pf, c2);
+}
 
 // ---------------------------------------------------------------- end of step
 // diag_flux() for the global region's inner x1 face (diag.c:576-833): the

@@ -8,13 +8,14 @@
 
 namespace harm {
 
-void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pb)
+void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a,
+                       const CUtensorMap& prim_map)
 {
   if (ffde) {
-    if (para) flux_rows_launch<float, true, true>(g, b, s, a, pb);
-    else flux_rows_launch<float, false, true>(g, b, s, a, pb);
-  } else if (para) flux_rows_launch<float, true, false>(g, b, s, a, pb);
-  else flux_rows_launch<float, false, false>(g, b, s, a, pb);
+    if (para) flux_rows_launch<float, true, true>(g, b, s, a, prim_map);
+    else flux_rows_launch<float, false, true>(g, b, s, a, prim_map);
+  } else if (para) flux_rows_launch<float, true, false>(g, b, s, a, prim_map);
+  else flux_rows_launch<float, false, false>(g, b, s, a, prim_map);
 }
 
 void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv)
@@ -22,11 +23,11 @@ void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const d
   k_emf<float><<<g, b, 0, s>>>(a, pv);
 }
 
-void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pi,
-                         const double* pb, double* pf, double c2)
+void launch_update_mixed(int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map,
+                         const double* pi, const double* pb, double* pf, double c2)
 {
-  if (ffde) k_update<float, true><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
-  else k_update<float, false><<<g, b, 0, s>>>(a, pi, pb, pf, c2);
+  if (ffde) update_launch<float, true>(g, b, s, a, map, pi, pb, pf, c2);
+  else update_launch<float, false>(g, b, s, a, map, pi, pb, pf, c2);
 }
 
 }  // namespace harm
