@@ -242,38 +242,56 @@ HD_INLINE T mc_slope(T yl, T yc, T yr)
   return minmod(Dqc, minmod(Dqm, Dqp));
 }
 
-// para4 with the MC sub-limiter, interp.c:444-538
+// para4 with the MC sub-limiter, interp.c:444-538, in its three parts.  A
+// zone's two raw interface values and the slopes they use are functions of
+// the values they sit between, the same whichever zone's para4 evaluates
+// them (the reference's operand order kept), so neighbouring zones may
+// share them; the limiting is the zone's own.
+// the MC-limited slope at y0 between ym and yp (the loop body)
 template <typename T>
-HD_INLINE void para4(T y0, T y1, T y2, T y3, T y4, T& lout, T& rout)
+HD_INLINE T para_dq(T ym, T y0, T yp)
 {
-  T y[5] = {y0, y1, y2, y3, y4}, dq[5];
-#pragma unroll
-  for (int i = 1; i < 4; i++) {
-    T Dqm = T(2.0) * (y[i] - y[i - 1]);
-    T Dqp = T(2.0) * (y[i + 1] - y[i]);
-    T Dqc = T(0.5) * (y[i + 1] - y[i - 1]);
-    T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
-    T s = Dqm * Dqp;
-    dq[i] = (s <= T(0.)) ? T(0.) : rmin(aDqc, rmin(aDqm, aDqp)) * rsign(Dqc);
-  }
-  T l = T(0.5) * (y[2] + y[1]) - (dq[2] - dq[1]) / T(8.0);
-  T r = T(0.5) * (y[3] + y[2]) - (dq[3] - dq[2]) / T(8.0);
-  l = rmax(rmin(y[2], y[1]), l);
-  l = rmin(rmax(y[2], y[1]), l);
-  r = rmax(rmin(y[2], y[3]), r);
-  r = rmin(rmax(y[2], y[3]), r);
-  T qa = (r - y[2]) * (y[2] - l);
+  T Dqm = T(2.0) * (y0 - ym);
+  T Dqp = T(2.0) * (yp - y0);
+  T Dqc = T(0.5) * (yp - ym);
+  T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
+  T s = Dqm * Dqp;
+  return (s <= T(0.)) ? T(0.) : rmin(aDqc, rmin(aDqm, aDqp)) * rsign(Dqc);
+}
+// the raw interface value between a lower zone (value ylo, slope dlo) and
+// an upper one (yhi, dhi)
+template <typename T>
+HD_INLINE T para_face(T ylo, T yhi, T dlo, T dhi)
+{
+  return T(0.5) * (yhi + ylo) - (dhi - dlo) / T(8.0);
+}
+// the zone value y's limited left and right states from its raw interface
+// values l (lower side, toward ym) and r (upper side, toward yp)
+template <typename T>
+HD_INLINE void para_limit(T ym, T y, T yp, T l, T r, T& lout, T& rout)
+{
+  l = rmax(rmin(y, ym), l);
+  l = rmin(rmax(y, ym), l);
+  r = rmax(rmin(y, yp), r);
+  r = rmin(rmax(y, yp), r);
+  T qa = (r - y) * (y - l);
   T qd = (r - l);
-  T qe = T(8.0) * (y[2] - T(0.5) * (l + r));
+  T qe = T(8.0) * (y - T(0.5) * (l + r));
   if (qa <= T(0.)) {
-    l = y[2];
-    r = y[2];
+    l = y;
+    r = y;
   } else {
-    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y[2] - T(2.0) * r;
-    if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y[2] - T(2.0) * l;
+    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y - T(2.0) * r;
+    if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y - T(2.0) * l;
   }
   lout = l;
   rout = r;
+}
+template <typename T>
+HD_INLINE void para4(T y0, T y1, T y2, T y3, T y4, T& lout, T& rout)
+{
+  const T d1 = para_dq(y0, y1, y2), d2 = para_dq(y1, y2, y3), d3 = para_dq(y2, y3, y4);
+  para_limit(y1, y2, y3, para_face(y1, y2, d1, d2), para_face(y2, y3, d2, d3), lout, rout);
 }
 
 // Deterministic Newton cycle-break factor in [0,1): splitmix64 finaliser

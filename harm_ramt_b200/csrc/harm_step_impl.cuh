@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
 {
   extern __shared__ __align__(128) double tile[];
   __shared__ double sh[2][32];
-  __shared__ T shr[NPR][BY][32];
+  __shared__ T shr[NPR][PARA ? 1 : BY][32];
   __shared__ uint64_t bar;
   const int tx = threadIdx.x, ty = threadIdx.y;
   constexpr int ROWS = flux_tile_rows(BY), PS = ROWS * FLUX_TILE_W;
@@ -191,16 +191,71 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
     for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
   }
   // ---- x2 faces
-  zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
+  if constexpr (PARA) {
+    // PPM along x2 with each slope and each raw interface value formed once
+    // for the block (para_dq, para_face) in shared memory after the tile:
+    // slopes at tile rows 1 .. BY+3 (every warp its own zone row, warps 0-2
+    // one more), raw values below tile rows 2 .. BY+3 (warps 0-1 one more),
+    // then every zone limits its own two (para_limit)
+    T* dq2 = reinterpret_cast<T*>(tile + NPR * PS);
+    T* fv2 = dq2 + NPR * (BY + 3) * 32;
+    const double* tc = tz - (ty + 3) * FLUX_TILE_W;  // the zone's column, tile row 0
+    auto dq_row = [&](int r) {
 #pragma unroll
-  for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
-  __syncthreads();
-  if (ty > 0) {
+      for (int k = 0; k < NPR; k++) {
+        const double* c = tc + k * PS + r * FLUX_TILE_W;
+        dq2[(k * (BY + 3) + r - 1) * 32 + tx] = para_dq((T)c[-FLUX_TILE_W], (T)c[0], (T)c[FLUX_TILE_W]);
+      }
+    };
+    dq_row(ty + 3);
+    if (ty < 2) dq_row(ty + 1);
+    else if (ty == 2) dq_row(BY + 3);
+    __syncthreads();
+    auto fv_row = [&](int r) {
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
+      for (int k = 0; k < NPR; k++) {
+        const double* c = tc + k * PS + r * FLUX_TILE_W;
+        const T* d = dq2 + (k * (BY + 3) + r - 1) * 32 + tx;
+        fv2[(k * (BY + 2) + r - 2) * 32 + tx] = para_face((T)c[-FLUX_TILE_W], (T)c[0], d[-32], d[0]);
+      }
+    };
+    fv_row(ty + 3);
+    if (ty == 0) fv_row(2);
+    else if (ty == 1) fv_row(BY + 3);
+    __syncthreads();
+    auto limit_row = [&](int r, T* Lo, T* Ro) {
+#pragma unroll
+      for (int k = 0; k < NPR; k++) {
+        const double* c = tc + k * PS + r * FLUX_TILE_W;
+        const T* f = fv2 + (k * (BY + 2) + r - 2) * 32 + tx;
+        para_limit((T)c[-FLUX_TILE_W], (T)c[0], (T)c[FLUX_TILE_W], f[0], f[32], Lo[k], Ro[k]);
+      }
+    };
+    limit_row(ty + 3, L, R);
+    // the slopes are read; their space takes the right states for the row above
+    T* shx = dq2;
+#pragma unroll
+    for (int k = 0; k < NPR; k++) shx[(k * BY + ty) * 32 + tx] = R[k];
+    __syncthreads();
+    if (ty > 0) {
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pl[k] = shx[(k * BY + ty - 1) * 32 + tx];
+    } else {
+      T Lm[NPR];
+      limit_row(2, Lm, pl);
+    }
   } else {
-    T Lm[NPR];
-    zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
+    zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
+    __syncthreads();
+    if (ty > 0) {
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
+    } else {
+      T Lm[NPR];
+      zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
+    }
   }
   if (in && j >= 0 && own) {
     face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
@@ -229,13 +284,15 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
 template <typename T, bool PARA, bool FFDE, int BY>
 inline void flux_launch_by(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map)
 {
+  // the tile, and for PPM the x2 slopes (BY + 3 rows) and raw interface
+  // values (BY + 2 rows) of 32 columns
+  constexpr size_t sm = flux_tile_bytes(BY) + (PARA ? (size_t)NPR * (2 * BY + 5) * 32 * sizeof(T) : 0);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_flux<T, PARA, FFDE, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_tile_bytes(BY));
+    cudaFuncSetAttribute(k_flux<T, PARA, FFDE, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = true;
   }
-  k_flux<T, PARA, FFDE, BY><<<g, b, flux_tile_bytes(BY), s>>>(a, map);
+  k_flux<T, PARA, FFDE, BY><<<g, b, sm, s>>>(a, map);
 }
 template <typename T, bool PARA, bool FFDE>
 inline void flux_rows_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map)
