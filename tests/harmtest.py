@@ -43,6 +43,81 @@ def build_oracle(force=False):
     return ORACLE_LIB
 
 
+ORACLE_TL_SRC = os.path.join(ORACLE_DIR, "harm_oracle_tl.cpp")
+ORACLE_TL_LIB = os.path.join(ORACLE_DIR, "libharm_oracle_tl.so")
+
+
+def build_oracle_tl(force=False):
+    """Compiles the tangent-linear form of the oracle (harm_oracle.c with a
+    dual-number type, oracle/harm_oracle_tl.cpp), no FP contraction."""
+    deps = [ORACLE_TL_SRC, ORACLE_SRC, os.path.join(ORACLE_DIR, "harm_oracle.h")]
+    if not force and os.path.exists(ORACLE_TL_LIB) and all(os.path.getmtime(ORACLE_TL_LIB) >= os.path.getmtime(d)
+                                                           for d in deps):
+        return ORACLE_TL_LIB
+    tmp = ORACLE_TL_LIB + ".tmp%d" % os.getpid()
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-o", tmp,
+                    ORACLE_TL_SRC, "-lm"], check=True, cwd=ORACLE_DIR)
+    os.replace(tmp, ORACLE_TL_LIB)
+    return ORACLE_TL_LIB
+
+
+class OracleTL:
+    """The oracle's step in forward mode: a state and one tangent."""
+
+    def __init__(self, n1, n2, geom, *, lim=3, fluxmethod=1, cour=0.8, gam=4.0 / 3.0, dx1, dx2, safe=1.3,
+                 defcon=1.0, gammamax=25.0, gammafail=2500.0, bsqorholimit=20.0, bsqoulimit=100.0, tf=1e30, eom=0,
+                 bc=0, omegastar=0.0, fluxadjust=0, gammadamp=5.0):
+        lib = ctypes.CDLL(build_oracle_tl())
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        lib.tl_create.restype = vp
+        lib.tl_create.argtypes = [ctypes.POINTER(OracleConfig), dp, dp, dp, dp, dp]
+        lib.tl_destroy.argtypes = [vp]
+        lib.tl_bound.argtypes = [vp, dp, dp]
+        lib.tl_step.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.c_double, ctypes.c_double]
+        lib.tl_horizon.argtypes = [vp, dp, dp]
+        self.lib = lib
+        self.cfg = OracleConfig(n1, n2, lim, fluxmethod, eom, cour, gam, dx1, dx2, safe, defcon, gammamax, gammafail,
+                                bsqorholimit, bsqoulimit, tf, bc, omegastar, fluxadjust, gammadamp)
+        g = {k: np.ascontiguousarray(geom[k], dtype=np.float64) for k in ("gcov", "gcon", "gdet", "conn", "floors")}
+        self.h = lib.tl_create(ctypes.byref(self.cfg), _dp(g["gcov"]), _dp(g["gcon"]), _dp(g["gdet"]), _dp(g["conn"]),
+                               _dp(g["floors"]))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.tl_destroy(self.h)
+            self.h = None
+
+    def bound(self, p, dp):
+        self.lib.tl_bound(self.h, _dp(p), _dp(dp))
+
+    def step(self, p, dp, pflag, t, dt):
+        return self.lib.tl_step(self.h, _dp(p), _dp(dp), pflag.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), t, dt)
+
+    def horizon(self):
+        v, d = np.zeros(6), np.zeros(6)
+        self.lib.tl_horizon(self.h, _dp(v), _dp(d))
+        return v, d
+
+    def objective(self, p0, v, dts, wm=1.0, we=1.0):
+        """J = sum_n dt_n (wm mdot_n + we edot_n) of the run from p0 (ghosts
+        refilled by bound_prim) with the dt sequence dts, and its derivative
+        along v (active zones)"""
+        p = np.ascontiguousarray(p0, dtype=np.float64).copy()
+        dp = np.ascontiguousarray(v, dtype=np.float64).copy()
+        self.bound(p, dp)
+        f = np.zeros(p.shape[:2] + (5,), dtype=np.int32)
+        J = dJ = 0.0
+        t = 0.0
+        for dt in dts:
+            rc = self.step(p, dp, f, t, float(dt))
+            assert rc == 0, rc
+            t += float(dt)
+            hv, hd = self.horizon()
+            J += float(dt) * (wm * hv[0] + we * (hv[2] + hv[3]))
+            dJ += float(dt) * (wm * hd[0] + we * (hd[2] + hd[3]))
+        return J, dJ, p, dp
+
+
 _oracle = None
 
 

@@ -99,8 +99,9 @@ def test_ffde_dipole_512x256_mc_laxf_10_steps(harm):
         pytest.skip("reference build (oracle/_ref) of the 512x256 dipole not present")
     cfg = ht.ref_config(r)
     o = ht.Oracle(n1, n2, r["geom"], lim=lim, fluxmethod=flux, eom=1, bc=1, omegastar=r["omegastar"], **cfg)
-    h = harm.HarmGPU(n1, n2, cfg.pop("dx1"), cfg.pop("dx2"), lim=lim, fluxmethod=flux, eom=harm.EOM_FFDE,
-                     bc=harm.BC_STAR, omegastar=r["omegastar"], **cfg)
+    rest = {k: v for k, v in cfg.items() if k not in ("dx1", "dx2")}
+    h = harm.HarmGPU(n1, n2, cfg["dx1"], cfg["dx2"], lim=lim, fluxmethod=flux, eom=harm.EOM_FFDE,
+                     bc=harm.BC_STAR, omegastar=r["omegastar"], **rest)
     g = r["geom"]
     h.upload_geometry(g["gcov"], g["gcon"], g["gdet"], g["conn"], g["floors"])
     h.set_prims(r["prims"][0], r["pflag"][0])
@@ -117,3 +118,48 @@ def test_ffde_dipole_512x256_mc_laxf_10_steps(harm):
         assert (st["t"], st["dt"]) == (t, dt)
     assert list(h.get_horizon().values()) == list(o.horizon())
     h.close()
+    _ffde_throughput(harm, r, cfg)
+
+
+def _ffde_throughput(harm, r, cfg):
+    """C2 at its size: zone-cycles/s of the dipole at 512 x 256 in FP64 and
+    in the mixed form (steps 201-400 from the reference's init, CUDA events
+    on the context's stream), the mixed-vs-FP64 differences at the end, and
+    the force-free constraints of the FP64 state: E.B = 0 holds by
+    construction (the inversion forms E = -v x B), E < B is the cap on the
+    drift Lorentz factor (AVOIDUTINF 2), reported as the share of zones at
+    the cap."""
+    import torch
+    n1, n2 = r["n1"], r["n2"]
+    g = r["geom"]
+    stream = torch.cuda.current_stream()
+    out = {}
+    for prec in (harm.PREC_FP64, harm.PREC_MIXED):
+        h = harm.HarmGPU(n1, n2, cfg["dx1"], cfg["dx2"], lim=3, fluxmethod=0, eom=harm.EOM_FFDE, bc=harm.BC_STAR,
+                         omegastar=r["omegastar"], precision=prec, stream=stream.cuda_stream,
+                         **{k: v for k, v in cfg.items() if k not in ("dx1", "dx2")})
+        h.upload_geometry(g["gcov"], g["gcon"], g["gdet"], g["conn"], g["floors"])
+        h.set_prims(r["prims"][0], r["pflag"][0])
+        h.set_time(r["times"][0][0], r["times"][0][1], 0)
+        h.step_ch(200)
+        h.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.step_ch(200)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 200
+        st = h.sync()
+        p, _ = h.get_prims()
+        out[prec] = (ms, p[3:-3, 3:-3], st)
+        h.close()
+    (m64, p64, s64), (mmx, pmx, smx) = out[harm.PREC_FP64], out[harm.PREC_MIXED]
+    assert s64["t"] > 0 and np.isfinite(pmx).all()
+    l1 = lambda a, b: float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+    gc = g["gcov"][3:-3, 3:-3, 3, 1:4, 1:4]
+    u = p64[..., 2:5]
+    gamma = np.sqrt(1.0 + np.einsum("...i,...ij,...j->...", u, gc, u))
+    print(f"\nC2 dipole {n1}x{n2}, steps 201-400: FP64 {n1 * n2 / (m64 * 1e-3):.3e} zone-cycles/s ({m64:.4f} ms/step), "
+          f"mixed {n1 * n2 / (mmx * 1e-3):.3e} ({mmx:.4f} ms/step, {m64 / mmx:.2f}x); mixed vs FP64 at t={s64['t']:.4g}: "
+          f"L1 B {l1(pmx[..., 5:8], p64[..., 5:8]):.2e}, u~ {l1(pmx[..., 2:5], p64[..., 2:5]):.2e}; "
+          f"zones at the drift Lorentz cap (E -> B): {(gamma > 25.0 * (1 - 1e-9)).mean():.4f}")
