@@ -14,7 +14,7 @@ the state afterwards (``torus_context`` / ``set_prims``).
 # k_update's width must be even (its TMA box starts on an even column)
 UPDATE_CANDIDATES = ((32, 4), (64, 2), (128, 1), (16, 8), (32, 2))
 SMALL_CANDIDATES = ((32, 4), (32, 8), (64, 4), (128, 2), (64, 2))
-SMALL_KERNELS = ("k_bsqflags", "k_emf", "k_bound", "k_poledeath", "k_gammacheck", "k_checksol", "k_checksol_serial",
+SMALL_KERNELS = ("k_bsqflags", "k_emf", "k_bound", "k_poledeath", "k_gammacheck", "k_checksol",
                  "k_fixup_compute", "k_bound_fix")
 
 _cache = {}

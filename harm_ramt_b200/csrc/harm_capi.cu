@@ -28,11 +28,11 @@ __global__ void k_bsqflags(StepArgs a, const double* pv);
 __global__ void k_bound(StepArgs a, double* pv, int with_pflag);
 __global__ void k_poledeath(StepArgs a, double* pv);
 __global__ void k_gammacheck(StepArgs a, double* pv, int poledeath);
-__global__ void k_checksol(StepArgs a, const double* pv, int round);
-__global__ void k_checksol_serial(StepArgs a, const double* pv, int nrounds);
+__global__ void k_bound_gc(StepArgs a, double* pv);
+__global__ void k_checksol(StepArgs a, double* pv, int poledeath);
+__global__ void k_checksol_rounds(StepArgs a, const double* pv);
 __global__ void k_fixup_compute(StepArgs a, const double* pv);
 __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd);
-__global__ void k_bound_fix(StepArgs a, double* pv);
 __global__ void k_faraday(StepArgs a, const double* pv);
 __global__ void k_current(StepArgs a);
 __global__ void k_currents_commit(StepArgs a);
@@ -65,7 +65,6 @@ __global__ void k_planes_to_ref(StepArgs a, const double* pv, double* ref, int* 
 
 using namespace harm;
 
-static const int CHK_ROUNDS = 4;
 
 struct harm_ctx {
   harm_config cfg;
@@ -195,7 +194,7 @@ enum { KC_BSQ = 0, KC_FLUX, KC_EMF, KC_UPDATE, KC_BOUND, KC_POLE, KC_GCHECK, KC_
 // (KC_FIXA: k_fixup_apply on the adjoint's recording path, k_bound_fix --
 // repairs, second bound and POLEDEATH in one kernel -- on every other)
 static const char* const KC_NAMES[KC_COUNT] = {"k_bsqflags", "k_flux", "k_emf", "k_update", "k_bound", "k_poledeath",
-                                               "k_gammacheck", "k_checksol", "k_checksol_serial", "k_fixup_compute",
+                                               "k_gammacheck", "k_checksol", "k_checksol_rounds", "k_fixup_compute",
                                                "k_bound_fix", "k_step_end", "k_horizon", "k_faraday",
                                                "k_current"};
 
@@ -245,16 +244,22 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
   cudaStream_t s = c->stream;
   const size_t pbytes = (size_t)NPR * c->gr.plane * sizeof(double), fbytes = (size_t)c->gr.plane * sizeof(int);
   if (rec) cudaMemcpyAsync(rec->pn, c->d_p, pbytes, cudaMemcpyDeviceToDevice, s);
-  // b^2 flags of the step's p: FP64 GRMHD sets them inside the first
-  // substep, the active zones' in k_update (from the state it forms anyway)
-  // and the one-zone ring's in k_emf; otherwise k_bsqflags first.  (With the
-  // flux switch every flag of the DQZLOOP range is needed before the first
-  // substep's fluxes, so they all come from k_bsqflags.)
-  const bool fuse_bsq = (c->cfg.precision == HARM_PREC_FP64) && (c->cfg.eom == HARM_EOM_GRMHD) && !c->cfg.fluxadjust;
-  if (!fuse_bsq) {
+  // b^2 flags of the step's p: GRMHD sets them inside the first substep,
+  // the active zones' in k_update (from the state it forms anyway) and the
+  // one-zone ring's in k_emf (in the mixed form these FP64 flags are built
+  // with contraction, like the rest of its kernels); the force-free step
+  // has none (k_bsqflags clears them).  (With the
+  // flux switch every flag of the DQZLOOP range is needed by the first
+  // substep's fluxes: each k_flux thread forms its zone's, which its faces
+  // use.)
+  const bool fuse_bsq = (c->cfg.eom == HARM_EOM_GRMHD) && !c->cfg.fluxadjust;
+  // with the switch, the first substep's k_flux forms all of them
+  const bool flags_in_flux = c->cfg.fluxadjust != 0;
+  if (!fuse_bsq && !flags_in_flux) {
     k_bsqflags<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, c->d_p);
     T.mark(s, KC_BSQ);
   }
+  bool step_ended = false;
   for (int sub = 0; sub < 2; sub++) {
     if (rec) {
       a.rec_pinv = rec->pinv[sub];
@@ -262,6 +267,7 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     }
     a.bsqf_fused = (fuse_bsq && sub == 0) ? a0.bsqf : nullptr;
     a.phase0 = sub * PH_PER_SUBSTEP;
+    a.flags_here = (flags_in_flux && sub == 0) ? 1 : 0;
     const double* pi = c->d_p;
     const double* pb = (sub == 0) ? c->d_p : c->d_pk0;
     double* pf = (sub == 0) ? c->d_pk0 : c->d_p;
@@ -280,6 +286,25 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
       cudaMemcpyAsync(rec->upd[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
       cudaMemcpyAsync(rec->flaginv[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
     }
+    if (!ffde && !rec) {
+      // GRMHD: the first bound with the check-solution gamma table, the vote
+      // (which also writes the POLEDEATH zeroing that follows this bound),
+      // its later rounds, the repairs, and the repairs applied with the
+      // second bound -- after the last substep also the end of the step
+      const bool last = (sub == 1) && !c->cfg.currents;
+      k_bound_gc<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf);
+      T.mark(s, KC_BOUND);
+      k_checksol<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, poledeath ? 1 : 0);
+      T.mark(s, KC_CHECKSOL);
+      k_checksol_rounds<<<1, 1024, 0, s>>>(a, pf);
+      T.mark(s, KC_CHECKSERIAL);
+      k_fixup_compute<<<grid2(n1, n2, b), b, 0, s>>>(a, pf);
+      T.mark(s, KC_FIXC);
+      launch_bound_fix(mixed, grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, s, a, pf, last ? 1 : 0);
+      T.mark(s, KC_FIXA);
+      if (last) step_ended = true;
+      continue;
+    }
     k_bound<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf, 1);
     T.mark(s, KC_BOUND);
     // force-free: no b^2 flags (so no check-solution votes) and no
@@ -292,26 +317,18 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
       if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
       continue;
     }
-    // the POLEDEATH zeroing after this bound is applied inside k_gammacheck
+    // the adjoint's recording keeps the states between the bounds, the
+    // zeroing and the repairs, so it runs them as separate kernels (the
+    // POLEDEATH zeroing after the first bound inside k_gammacheck)
     k_gammacheck<<<grid2(n1 + 2, n2 + 2, b), b, 0, s>>>(a, pf, poledeath ? 1 : 0);
     T.mark(s, KC_GCHECK);
-    if (rec) cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
-    for (int r = 0; r < CHK_ROUNDS; r++) {
-      k_checksol<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, r);
-      T.mark(s, KC_CHECKSOL);
-    }
-    k_checksol_serial<<<1, 32, 0, s>>>(a, pf, CHK_ROUNDS);
+    cudaMemcpyAsync(rec->snap[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
+    k_checksol<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, 0);
+    T.mark(s, KC_CHECKSOL);
+    k_checksol_rounds<<<1, 1024, 0, s>>>(a, pf);
     T.mark(s, KC_CHECKSERIAL);
     k_fixup_compute<<<grid2(n1, n2, b), b, 0, s>>>(a, pf);
     T.mark(s, KC_FIXC);
-    if (!rec) {
-      // repairs applied, second bound, POLEDEATH: one kernel
-      k_bound_fix<<<grid2(n1 + 2 * NG, n2 + 2 * NG, b), b, 0, s>>>(a, pf);
-      T.mark(s, KC_FIXA);
-      continue;
-    }
-    // the adjoint's recording keeps the state between the repairs and the
-    // second bound, so it runs them as separate kernels
     k_fixup_apply<<<grid2(n1, n2, b), b, 0, s>>>(a, pf, 1);
     cudaMemcpyAsync(rec->pre2[sub], pf, pbytes, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(rec->flag[sub], c->d_pflag, fbytes, cudaMemcpyDeviceToDevice, s);
@@ -328,9 +345,11 @@ static int enqueue_step(harm_ctx* c, Timer* tm = nullptr, const Rec* rec = nullp
     k_currents_commit<<<1, 1, 0, s>>>(a);
     T.mark(s, KC_CURRENT, 2);
   }
-  // horizon accounting and the new dt
-  launch_step_end(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
-  T.mark(s, KC_DT);
+  // horizon accounting and the new dt (unless the last k_bound_fix did it)
+  if (!step_ended) {
+    launch_step_end(c->cfg.precision == HARM_PREC_MIXED, s, a, c->d_p);
+    T.mark(s, KC_DT);
+  }
   return cudaGetLastError() == cudaSuccess ? HARM_OK : HARM_ECUDA;
 }
 

@@ -347,18 +347,28 @@ HD_INLINE void func_vsq(const U2PCtx& c, double W, double vsq, double& dx0, doub
 
 // general_newton_raphson + validate_x(vartype 3), utoprim_2d.c:606-740, 556-600
 // Returns 0/1 as the reference does, or NEWTON_DEFERRED when `maxit` (< 200)
-// iterations ran without convergence; the caller then redoes the solve with
-// the full 200 (the iteration sequence is deterministic, so the redo reaches
-// the reference's result).
+// iterations ran without convergence.  The loop's whole state is then saved
+// to st[0], st[ss], ... st[4 ss] (x0, x1, errx, errx_old, iteration count)
+// when st is given, and a later call with `resume` set continues from it up
+// to the full 200: the iteration sequence is deterministic, so the split
+// solve reaches the reference's result with no iteration repeated.
 constexpr int NEWTON_DEFERRED = -7;
+constexpr int NEWTON_STATE = 5;
 __device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x1, double gammafail, int& niter_out,
-                                          int maxit)
+                                          int maxit, double* st, long long ss, bool resume)
 {
   constexpr int MAX_NEWT_ITER = 200;
   constexpr double NEWT_TOL = 1.0e-15, MIN_NEWT_TOL = 1.0e-10, W_TOO_BIG = 1.e9;
   const double vsq_too_big = (1.0 - 1.0 / (gammafail - 1.0));
   double errx = 1., errx_old = 2., errx_oldest;
   int n_iter = 0;
+  if (resume) {
+    x0 = st[0];
+    x1 = st[ss];
+    errx = st[2 * ss];
+    errx_old = st[3 * ss];
+    n_iter = (int)st[4 * ss];
+  }
   while ((errx > NEWT_TOL) && (n_iter < maxit)) {
     double dx0, dx1;
     func_vsq(c, x0, x1, dx0, dx1);
@@ -384,7 +394,16 @@ __device__ __forceinline__ int newton_vsq(const U2PCtx& c, double& x0, double& x
     n_iter++;
   }
   niter_out = n_iter;
-  if (maxit < MAX_NEWT_ITER && n_iter >= maxit && errx > NEWT_TOL) return NEWTON_DEFERRED;
+  if (maxit < MAX_NEWT_ITER && n_iter >= maxit && errx > NEWT_TOL) {
+    if (st) {
+      st[0] = x0;
+      st[ss] = x1;
+      st[2 * ss] = errx;
+      st[3 * ss] = errx_old;
+      st[4 * ss] = (double)n_iter;
+    }
+    return NEWTON_DEFERRED;
+  }
   if (n_iter >= MAX_NEWT_ITER) return (errx > MIN_NEWT_TOL) ? 1 : 0;
   return 0;
 }
@@ -471,9 +490,11 @@ HD_INLINE void lower_g(const double* v, const double* c, double* w)
 // Utoprimgen(UEVOLVE) -> UtoU -> Utoprim_2d -> Utoprim_new_body:
 // step_ch.c:468-552, phys.c:219-265, utoprim_2d.c:25-310.  U is the evolved
 // conserved vector (with sqrt(-g)); pr holds the guess on entry.  Returns
-// the pflag code; *niter gets the Newton iteration count.
+// the pflag code; *niter gets the Newton iteration count.  nst, nss, resume:
+// the Newton state of a deferred solve (newton_vsq), or null.
 __device__ __forceinline__ int utoprim_2d(const double* U, const Geo<double>& g, double* pr, double gam, double gammafail,
-                                          int* niter, int maxit = 200)
+                                          int* niter, int maxit = 200, double* nst = nullptr, long long nss = 0,
+                                          bool resume = false)
 {
   constexpr double W_TOO_BIG = 1.e9, FAIL_VAL = 1.e30;
   double Ug[NPR], Ut[NPR], pt[NPR];
@@ -530,7 +551,7 @@ __device__ __forceinline__ int utoprim_2d(const double* U, const Geo<double>& g,
       c.wglobal = w;
       double x0 = fabs(W), ut = fabs(utsq_calc(c, W));
       double x1 = (ut > 0.) ? (ut / (ut + 1.)) : 0.0;
-      int ret = newton_vsq(c, x0, x1, gammafail, *niter, maxit);
+      int ret = newton_vsq(c, x0, x1, gammafail, *niter, maxit, nst, nss, resume);
       if (ret == NEWTON_DEFERRED) return NEWTON_DEFERRED;
       if (ret != 0) {
         pfl = ret * 100 + 1;

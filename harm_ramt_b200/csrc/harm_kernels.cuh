@@ -61,8 +61,7 @@ struct DevScalars {
   long long realnstep;
   unsigned long long fail_inv;  // ~key of the first fatal check in the reference's order (0 = none; see fail_key)
   unsigned long long newton_iters;   // Newton iterations since the last reset
-  int chk_changed[8];    // per-round change flags of the check-solution sweep
-  int chk_final;         // last round that wrote its decisions (buffer chk_final & 1)
+  int nchk;              // check-solution zones whose vote may change after round 0 (this substep)
   int fixups;            // zones repaired by fixup_utoprim since the last harm_set_time
   double hz[7];          // horizon accounting of the last step (see k_step_end); hz[6]:
                          // sum of dt (b^2 u^r u_t - b^r b_t) terms since the last harm_set_time
@@ -71,7 +70,8 @@ struct DevScalars {
   int cur_ring;          // currents: ring level holding the newest F^{i t}
   long long ccalls;      // currents: calls of current_calc_1 (its static count)
   double clastdt;        // currents: dt of the previous call (its static lastdt)
-  int chk_multi;         // substeps whose check-solution sweep ran more than one round
+  int chk_multi;         // substeps whose check-solution sweep needed rounds after the first
+  unsigned blocks_done;  // blocks of k_bound_fix finished (its last block ends the step; reset by that block)
 };
 
 struct StepArgs {
@@ -98,6 +98,7 @@ struct StepArgs {
   unsigned char* rec_fixset;  // adjoint recording (or null): neighbour set of each repaired zone
   int nblocks_flux;
   int phase0;            // PH_PER_SUBSTEP * substep: the fail-key phase of this launch's substep
+  int flags_here;        // k_flux forms every zone's b^2 flags and flux choice (the first substep, FP64, fluxadjust)
   DevScalars* sc;
 };
 
@@ -180,7 +181,10 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
 // 4 rows (four 128-thread blocks per SM) on smaller grids.  The FP32 faces
 // of the mixed form fit 128 registers without spilling and run best as
 // 4-row blocks at four per SM on any grid.
-constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = 16;
+#ifndef HARM_FLUX_BY_LARGE
+#define HARM_FLUX_BY_LARGE 16
+#endif
+constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = HARM_FLUX_BY_LARGE;
 // k_flux's primitive tile (one TMA box over a state's 8 planes): the 32
 // columns of the block's zones and 2 more on each side (PARA's stencil) = 36,
 // starting on the even column at or before the first (TMA copies start on
@@ -214,6 +218,7 @@ void launch_emf(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, co
 void launch_update(int mixed, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map,
                    const double* pi, const double* pb, double* pf, double c2);
 void launch_step_end(int mixed, cudaStream_t s, const StepArgs& a, const double* pv);
+void launch_bound_fix(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, double* pv, int step_end);
 void launch_flux_mixed(int para, int ffde, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a,
                        const CUtensorMap& prim_map);
 void launch_emf_mixed(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const double* pv);

@@ -9,7 +9,8 @@
 //   k_bound        bound_prim + bound_pflag (ghost zones only)
 //   k_poledeath    the POLEDEATH zeroing of the first/last active x2 rows
 //   k_gammacheck,
-//   k_checksol     fixup_checksolution (parallel fixed-point sweep, exact)
+//   k_checksol,
+//   k_checksol_rounds  fixup_checksolution (parallel fixed-point sweep, exact)
 //   k_fixup_*      fixup_utoprim from a snapshot
 //   k_bound/k_poledeath again, and k_dt_finalize after the last substep.
 #include <cuda_runtime.h>
@@ -54,9 +55,11 @@ __global__ void k_bsqflags(StepArgs a, const double* __restrict__ pv)
   }
 }
 
-// The deferred inversions of k_update, redone with the full iteration limit.
+// The deferred inversions of k_update, continued from the Newton state
+// k_update saved (repair scratch planes 0-4) up to the full iteration limit.
 // A deferred zone's pf slot was not written, so pi still holds its guess.
-// TA: the UTOPRIMTRYAGAIN retry chain follows a failed 2D inversion.
+// TA: the UTOPRIMTRYAGAIN retry chain follows a failed 2D inversion (those
+// zones carry no saved state and are solved afresh).
 template <bool TA>
 __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __restrict__ pi, double* __restrict__ pf)
 {
@@ -74,7 +77,9 @@ __global__ void __launch_bounds__(64) k_update_tail(StepArgs a, const double* __
       pfz[k] = pi[k * pl + z];
     }
     int niter;
-    int pfl = utoprim_2d(U, g, pfz, a.pp.gam, a.pp.gammafail, &niter);
+    double* nst = a.fixbuf + z;
+    const bool resume = nst[(NEWTON_STATE - 1) * pl] >= 0.0;
+    int pfl = utoprim_2d(U, g, pfz, a.pp.gam, a.pp.gammafail, &niter, 200, nst, pl, resume);
     if (TA && pfl != 0) {
       double pr0[NPR];
 #pragma unroll
@@ -164,7 +169,7 @@ __device__ __forceinline__ double srcv(const StepArgs& a, const double* pv, long
 {
   const long long pl = a.gr.plane;
   if (APPLY && k <= U3) {
-    if (a.pflag[zs] != 0 || a.chk[(long long)(a.sc->chk_final & 1) * pl + zs] != 0) return a.fixbuf[k * pl + zs];
+    if (a.pflag[zs] != 0 || a.chk[zs] != 0) return a.fixbuf[k * pl + zs];
   }
   return pv[k * pl + zs];
 }
@@ -294,16 +299,22 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
 // repaired holds u~2 = B2 = 0 already (the first bound zeroed them and
 // nothing changed them since), so the ghosts read the same value before or
 // after it is rewritten; a repaired one is read from the repair buffer.
-__global__ void k_bound_fix(StepArgs a, double* pv)
+//
+// With step_end set (after the last substep) the grid carries extra rows of
+// blocks past the zones' (from block row `hrow0`): their threads form the
+// horizon terms of rows j from the final state of zone (0, j) -- the value
+// its own thread writes in this kernel: the repair buffer's or pv's, times
+// 0 for u~2 and B2 on the POLEDEATH rows (x * 0 of a value already zeroed
+// is the same zero) -- into ubuf, and the last block to finish runs
+// step_end_finish (the blocks count themselves in sc->blocks_done).
+__device__ __forceinline__ void bound_fix_zone(const StepArgs& a, double* pv, int i, int j)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
   const int n1 = a.gr.n1, n2 = a.gr.n2;
   if (i >= n1 + NG || j >= n2 + NG) return;
   if (i >= 0 && i < n1 && j >= 0 && j < n2) {
     const long long pl = a.gr.plane, z = a.gr.at(i, j);
     const int f = a.pflag[z];
-    const int c = a.chk[(long long)(a.sc->chk_final & 1) * pl + z];
+    const int c = a.chk[z];
     if (f != 0 || c != 0) {
 #pragma unroll
       for (int k = 0; k <= U3; k++) pv[k * pl + z] = a.fixbuf[k * pl + z];
@@ -317,6 +328,51 @@ __global__ void k_bound_fix(StepArgs a, double* pv)
     return;
   }
   bound_ghost<true>(a, pv, i, j, 0);
+}
+
+template <typename FT>
+__global__ void k_bound_fix(StepArgs a, double* pv, int step_end, int hrow0)
+{
+  if ((int)blockIdx.y < hrow0) {
+    bound_fix_zone(a, pv, blockIdx.x * blockDim.x + threadIdx.x - NG, blockIdx.y * blockDim.y + threadIdx.y - NG);
+  } else {
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int j = ((blockIdx.y - hrow0) * gridDim.x + blockIdx.x) * nt + tid;
+    if (j < a.gr.n2) {
+      const long long pl = a.gr.plane, z = a.gr.at(0, j);
+      double pr[NPR], t4[4];
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pr[k] = srcv<true>(a, pv, z, k);
+      if (a.pp.bc == 0 && (j == 0 || j == a.gr.n2 - 1)) {
+        pr[U2] *= 0.;
+        pr[B2] *= 0.;
+      }
+      horizon_terms<FT>(a, pr, j, t4);
+#pragma unroll
+      for (int k = 0; k < 4; k++) a.ubuf[k * pl + j] = t4[k];
+    }
+  }
+  if (!step_end) return;
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    __threadfence();
+    const unsigned nb = gridDim.x * gridDim.y;
+    last = (atomicAdd(&a.sc->blocks_done, 1u) == nb - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  step_end_finish<true>(a, a.ubuf, a.gr.plane);
+  if (threadIdx.x == 0 && threadIdx.y == 0) a.sc->blocks_done = 0;
+}
+
+void launch_bound_fix(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, double* pv, int step_end)
+{
+  const int hrow0 = (int)g.y;
+  if (step_end) g.y += (a.gr.n2 + g.x * b.x * b.y - 1) / (g.x * b.x * b.y);
+  if (mixed) k_bound_fix<float><<<g, b, 0, s>>>(a, pv, step_end, hrow0);
+  else k_bound_fix<double><<<g, b, 0, s>>>(a, pv, step_end, hrow0);
 }
 
 // POLEDEATH on the first and last active x2 rows (bounds.fishmon.c:296-327)
@@ -336,11 +392,56 @@ __global__ void k_poledeath(StepArgs a, double* pv)
 // applies the POLEDEATH zeroing of k_poledeath to its own zone (the bound
 // before this kernel has read those rows already; this kernel reads only
 // its own zone).
+// The first bound of a GRMHD substep with the gamma table of the check-
+// solution vote in one kernel: ghost zones are filled (bound_prim +
+// bound_pflag) and those of the one-zone ring set their gamma from the value
+// just formed; active zones of the DQZLOOP range set theirs from pv, with
+// the POLEDEATH zeroing of u~2 and B2 on the first and last rows applied to
+// the copy only -- the ghosts read those rows before the zeroing, as the
+// reference's bound does, so k_checksol writes it to pv (it reads only u of
+// its neighbours).
+__device__ __forceinline__ void gammacheck_set(const StepArgs& a, long long z, const double* pr)
+{
+  if (a.bsqf[z] == 0 || a.pflag[z] != 0) return;
+  Geo<double> g;
+  load_geo(a, CENT, z, g);
+  a.gammacheck[z] = gamma_of(pr, g);
+}
+
+__global__ void k_bound_gc(StepArgs a, double* pv)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - NG;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - NG;
+  const int n1 = a.gr.n1, n2 = a.gr.n2;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) a.sc->nchk = 0;
+  if (i >= n1 + NG || j >= n2 + NG) return;
+  const long long pl = a.gr.plane, z = a.gr.at(i, j);
+  const bool ring = i >= -1 && i <= n1 && j >= -1 && j <= n2;
+  if (i >= 0 && i < n1 && j >= 0 && j < n2) {
+    double pr[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
+    if (a.pp.bc == 0 && (j == 0 || j == n2 - 1)) {
+      pr[U2] *= 0.;
+      pr[B2] *= 0.;
+    }
+    gammacheck_set(a, z, pr);
+    return;
+  }
+  bound_ghost<false>(a, pv, i, j, 1);
+  if (ring) {
+    double pr[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
+    gammacheck_set(a, z, pr);
+  }
+}
+
 __global__ void k_gammacheck(StepArgs a, double* __restrict__ pv, int poledeath)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 8 && threadIdx.y == 0) a.sc->chk_changed[threadIdx.x] = 0;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) a.sc->nchk = 0;
   if (i > a.gr.n1 || j > a.gr.n2) return;
   const long long z = a.gr.at(i, j);
   if (poledeath && i >= 0 && i < a.gr.n1 && (j == 0 || j == a.gr.n2 - 1)) {
@@ -356,29 +457,17 @@ __global__ void k_gammacheck(StepArgs a, double* __restrict__ pv, int poledeath)
   a.gammacheck[z] = gamma_of(pr, g);
 }
 
-// One round of the check-solution vote.  The reference sweeps zones in ZLOOP
-// order (i outer, j inner) and a zone flagged there is seen as failed by the
-// zones after it.  Here every candidate is decided from the decisions of its
-// earlier neighbours in the previous round; the earlier-than relation is
-// acyclic, so the sweep's result is the unique fixed point and a round with
-// no change proves it has been reached.
-__global__ void k_checksol(StepArgs a, const double* __restrict__ pv, int round)
+// The check-solution vote of candidate zone (i, j) (fixup.c:402-482).  The
+// reference sweeps zones in ZLOOP order (i outer, j inner) and a zone it
+// flags is seen as failed by the zones after it: with `prev` given, an
+// earlier active neighbour whose decision there is nonzero counts as failed;
+// without, as the pflag says alone.  The neighbour list and the vote keep the
+// reference's form (its list names (+1, +1) twice and not (-1, +1); every
+// vote is gated on the first neighbour's ratio).
+__device__ __forceinline__ unsigned char checksol_vote(const StepArgs& a, const double* __restrict__ pv, int i, int j,
+                                                       long long z, const unsigned char* prev)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (round > 0 && !a.sc->chk_changed[round - 1]) return;
-  if (i == 0 && j == 0) {
-    a.sc->chk_final = round;
-    if (round == 1) a.sc->chk_multi++;
-  }
-  if (i >= a.gr.n1 || j >= a.gr.n2) return;
-  const long long z = a.gr.at(i, j), pl = a.gr.plane;
-  unsigned char* cur = a.chk + (long long)(round & 1) * pl;
-  const unsigned char* prev = a.chk + (long long)((round + 1) & 1) * pl;
-  if (a.bsqf[z] == 0 || a.pflag[z] != 0) {
-    cur[z] = 0;
-    return;
-  }
+  const long long pl = a.gr.plane;
   const int di[8] = {0, 0, 1, -1, 1, 1, 1, -1};
   const int dj[8] = {1, -1, 0, 0, 1, -1, 1, -1};
   const double g0 = a.gammacheck[z], u0 = pv[UU * pl + z];
@@ -388,9 +477,8 @@ __global__ void k_checksol(StepArgs a, const double* __restrict__ pv, int round)
     const int ii = i + di[l], jj = j + dj[l];
     const long long zz = a.gr.at(ii, jj);
     bool ok = (a.pflag[zz] == 0);
-    // an earlier (ZLOOP order) candidate neighbour counts as failed if flagged
     const bool earlier = (ii < i) || (ii == i && jj < j);
-    if (ok && round > 0 && earlier && ii >= 0 && ii < a.gr.n1 && jj >= 0 && jj < a.gr.n2 && prev[zz] != 0) ok = false;
+    if (ok && prev && earlier && ii >= 0 && ii < a.gr.n1 && jj >= 0 && jj < a.gr.n2 && prev[zz] != 0) ok = false;
     pd[l] = ok ? (a.gammacheck[zz] / g0) : -1;
     pd2[l] = ok ? (pv[UU * pl + zz] / u0) : -1;
   }
@@ -406,61 +494,88 @@ __global__ void k_checksol(StepArgs a, const double* __restrict__ pv, int round)
   unsigned char d = 0;
   if (v0 > nv * 0.5) d = PF_GAMMAPERC;
   if (v1 > nv * 0.5) d = PF_UPERC;
-  if (round > 0 && d != prev[z]) a.sc->chk_changed[round] = 1;
-  if (round == 0 && d != 0) {
-    // a flagged zone can only influence later candidates
-    bool later_cand = false;
-    const int li[4] = {0, 1, 1, 1}, lj[4] = {1, -1, 0, 1};
-#pragma unroll
-    for (int l = 0; l < 4; l++) {
-      const int ii = i + li[l], jj = j + lj[l];
-      if (ii < a.gr.n1 && jj >= 0 && jj < a.gr.n2) {
-        const long long zz = a.gr.at(ii, jj);
-        if (a.bsqf[zz] != 0 && a.pflag[zz] == 0) later_cand = true;
-      }
-    }
-    if (later_cand) a.sc->chk_changed[0] = 1;
-  }
-  cur[z] = d;
+  return d;
 }
 
-// Sequential ZLOOP sweep for the rare case where the rounds did not settle.
-__global__ void k_checksol_serial(StepArgs a, const double* __restrict__ pv, int nrounds)
+__device__ __forceinline__ bool checksol_candidate(const StepArgs& a, int i, int j)
 {
-  if (!a.sc->chk_changed[nrounds - 1]) return;
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const long long pl = a.gr.plane;
-  const int di[8] = {0, 0, 1, -1, 1, 1, 1, -1};
-  const int dj[8] = {1, -1, 0, 0, 1, -1, 1, -1};
-  a.sc->chk_final = nrounds - 1;
-  unsigned char* out = a.chk + (long long)((nrounds - 1) & 1) * pl;
+  if (i < 0 || i >= a.gr.n1 || j < 0 || j >= a.gr.n2) return false;
+  const long long z = a.gr.at(i, j);
+  return a.bsqf[z] != 0 && a.pflag[z] == 0;
+}
+
+// Round 0 of the sweep: every candidate voted as if no earlier zone were
+// flagged, into decision plane 0.  A vote can only lose counts when an
+// earlier neighbour is flagged (a failed neighbour's ratio of -1 counts no
+// vote), so the sweep's flagged set is a subset of round 0's, and only a
+// zone flagged here that has an earlier candidate neighbour (of its list:
+// (i, j-1), (i-1, j), (i-1, j-1)) can end differently: those go to the
+// worklist (the deferred-inversion list, idle by now) for k_checksol_rounds.
+// With poledeath set (after k_bound_gc) the thread of a zone on the first or
+// last row applies the POLEDEATH zeroing of u~2 and B2 to pv first.
+__global__ void k_checksol(StepArgs a, double* __restrict__ pv, int poledeath)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.gr.n1 || j >= a.gr.n2) return;
+  const long long z = a.gr.at(i, j);
+  if (poledeath && (j == 0 || j == a.gr.n2 - 1)) {
+    pv[U2 * a.gr.plane + z] *= 0.;
+    pv[B2 * a.gr.plane + z] *= 0.;
+  }
+  if (a.bsqf[z] == 0 || a.pflag[z] != 0) {
+    a.chk[z] = 0;
+    return;
+  }
+  const unsigned char d = checksol_vote(a, pv, i, j, z, nullptr);
+  a.chk[z] = d;
+  if (d != 0 && (checksol_candidate(a, i, j - 1) || checksol_candidate(a, i - 1, j) ||
+                 checksol_candidate(a, i - 1, j - 1)))
+    a.worklist[atomicAdd(&a.sc->nchk, 1)] = (int)z;
+}
+
+// The rest of the sweep, one block: the worklist zones re-vote from the
+// previous round's decisions of their earlier neighbours (plane 0), new
+// decisions staged in plane 1 (indexed by worklist slot) and copied back,
+// until a round changes nothing.  The earlier-than relation is acyclic, so
+// these rounds reach the sweep's unique fixed point within (longest chain of
+// worklist zones + 1) rounds; after CHK_MAX_ROUNDS without it (never seen)
+// thread 0 runs the reference's sweep itself over every zone.
+constexpr int CHK_MAX_ROUNDS = 64;
+__global__ void __launch_bounds__(1024) k_checksol_rounds(StepArgs a, const double* __restrict__ pv)
+{
+  const int nw = a.sc->nchk;
+  if (nw == 0) return;
+  if (threadIdx.x == 0) a.sc->chk_multi++;
+  unsigned char* d0 = a.chk;
+  unsigned char* dn = a.chk + a.gr.plane;
+  __shared__ int changed;
+  bool settled = false;
+  for (int r = 1; r <= CHK_MAX_ROUNDS; r++) {
+    if (threadIdx.x == 0) changed = 0;
+    __syncthreads();
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+      const long long z = a.worklist[w];
+      const int i = (int)(z % a.gr.pitch) - NG, j = (int)(z / a.gr.pitch) - NG;
+      const unsigned char d = checksol_vote(a, pv, i, j, z, d0);
+      dn[w] = d;
+      if (d != d0[z]) changed = 1;
+    }
+    __syncthreads();
+    if (!changed) {
+      settled = true;
+      break;
+    }
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) d0[a.worklist[w]] = dn[w];
+    __syncthreads();
+  }
+  if (settled || threadIdx.x != 0) return;
   for (int i = 0; i < a.gr.n1; i++)
     for (int j = 0; j < a.gr.n2; j++) {
       const long long z = a.gr.at(i, j);
-      out[z] = 0;
+      d0[z] = 0;
       if (a.bsqf[z] == 0 || a.pflag[z] != 0) continue;
-      const double g0 = a.gammacheck[z], u0 = pv[UU * pl + z];
-      double pd[8], pd2[8];
-      for (int l = 0; l < 8; l++) {
-        const int ii = i + di[l], jj = j + dj[l];
-        const long long zz = a.gr.at(ii, jj);
-        bool ok = (a.pflag[zz] == 0);
-        const bool earlier = (ii < i) || (ii == i && jj < j);
-        if (ok && earlier && ii >= 0 && jj >= 0 && jj < a.gr.n2 && out[zz] != 0) ok = false;
-        pd[l] = ok ? (a.gammacheck[zz] / g0) : -1;
-        pd2[l] = ok ? (pv[UU * pl + zz] / u0) : -1;
-      }
-      int v0 = 0, v1 = 0, nv = 0;
-      for (int l = 0; l < 8; l++)
-        if (pd[0] >= 0.0) {
-          if ((fabs(pd[l]) > 2.0) || (fabs(pd[l]) < 1.0 / 2.0)) v0++;
-          if ((fabs(pd2[l]) > 10.0) || (fabs(pd2[l]) < 1.0 / 10.0)) v1++;
-          nv++;
-        }
-      unsigned char d = 0;
-      if (v0 > nv * 0.5) d = PF_GAMMAPERC;
-      if (v1 > nv * 0.5) d = PF_UPERC;
-      out[z] = d;
+      d0[z] = checksol_vote(a, pv, i, j, z, d0);
     }
 }
 
@@ -473,7 +588,7 @@ __global__ void k_fixup_compute(StepArgs a, const double* __restrict__ pv)
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= a.gr.n1 || j >= a.gr.n2) return;
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
-  const unsigned char* chk = a.chk + (long long)(a.sc->chk_final & 1) * pl;
+  const unsigned char* chk = a.chk;
   int f = a.pflag[z];
   if (f == 0) f = chk[z];
   if (f == 0) return;
@@ -544,7 +659,7 @@ __global__ void k_fixup_apply(StepArgs a, double* pv, int grmhd)
   if (i >= a.gr.n1 || j >= a.gr.n2) return;
   const long long pl = a.gr.plane, z = a.gr.at(i, j);
   int f = a.pflag[z];
-  const int c = a.chk[(long long)(a.sc->chk_final & 1) * pl + z];
+  const int c = a.chk[z];
   if (f == 0 && c != 0) f = c;
   if (f == 0) return;
   if (grmhd) {

@@ -44,7 +44,7 @@ __device__ __forceinline__ void zone_states(const double* t, int ps, int st, T* 
 // left and the right wavespeeds) are the reference's.
 template <typename T, bool FFDE>
 __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int dir, T* p_l, T* p_r, T* Fo,
-                                          double& dtij)
+                                          double& dtij, int rf)
 {
   const long long z = a.gr.at(i, j);
   Geo<T> g;
@@ -84,10 +84,9 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   lmin = fabs(rmax(T(0.), -lmin));
   lmax = fabs(rmax(T(0.), lmax));
   T cmin = lmin, cmax = lmax, ctop = rmax(lmax, lmin);
-  // choose_flux, step_ch.c:703-738: fluxmethod, or with FLUXADJUST
-  // (HYDROFLUXADJUSTONLY 1) the hydro variables follow FLAGREALFLUX of zone
-  // (i, j), the face's own zone
-  const int rf = a.pp.fluxadjust ? (int)a.fluxf[z] : a.pp.fluxmethod;
+  // choose_flux, step_ch.c:703-738: rf is fluxmethod, or with FLUXADJUST
+  // (HYDROFLUXADJUSTONLY 1) FLAGREALFLUX of zone (i, j), the face's own
+  // zone, for the hydro variables
   if (cmax + cmin != T(0.0)) {
 #pragma unroll
     for (int k = 0; k < NPR; k++) {
@@ -148,7 +147,7 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
 {
   extern __shared__ __align__(128) double tile[];
   __shared__ double sh[2][32];
-  __shared__ T shr[NPR][PARA ? 1 : BY][32];
+  __shared__ T shr[NPR][BY][32];
   __shared__ uint64_t bar;
   const int tx = threadIdx.x, ty = threadIdx.y;
   constexpr int ROWS = flux_tile_rows(BY), PS = ROWS * FLUX_TILE_W;
@@ -178,12 +177,43 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
   // the zone's value of plane 0 in the tile: row ty + 3, column tx + 2 + (the
   // block's first column - cx)
   const double* tz = tile + (ty + 3) * FLUX_TILE_W + tx + 2 + ((int)(blockIdx.x * FLUX_BX) - cx);
+  // the flux choice of this zone, which both of its faces use: fluxmethod,
+  // or with the per-zone switch FLAGREALFLUX, formed here in the first
+  // substep of the FP64 step (from the step's p, which is this substep's
+  // tile; get_bsqflags, fixup.c:1197-1295, with the b^2 flags the repairs
+  // read later) and read back in the second
+  int rf = a.pp.fluxmethod;
+  if (a.pp.fluxadjust && in) {
+    if (a.flags_here) {
+      double pr[NPR];
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pr[k] = tz[k * PS];
+      Geo<double> gz;
+      load_geo(a, CENT, z, gz);
+      unsigned char b = 0;
+      if (!a.pp.eom) {
+        State<double> q;
+        state_of(pr, gz, q);
+        b = bsq_flag(a, pr, q);
+      }
+      const double gamma = gamma_of(pr, gz);
+      const int f1 = (gamma > 2.0 * a.pp.gammadamp) ? 2 : ((gamma > a.pp.gammadamp) ? 1 : 0);
+      rf = ((b & 3) == 2 || f1 == 2 || (b >> 2) == 2) ? a.pp.fluxmethod - 1 : a.pp.fluxmethod;
+      rf = (rf < 0) ? 0 : rf;
+      if (own) {
+        a.bsqf[z] = b;
+        a.fluxf[z] = (unsigned char)rf;
+      }
+    } else {
+      rf = (int)a.fluxf[z];
+    }
+  }
   // ---- x1 faces
   zone_states<T, PARA>(tz, PS, 1, L, R);
 #pragma unroll
   for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
   if (in && i >= 0 && tx > 0) {
-    face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij);
+    face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij, rf);
     dt1 = (dtij < dt1) ? dtij : dt1;
     if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
     if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
@@ -191,74 +221,19 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
     for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
   }
   // ---- x2 faces
-  if constexpr (PARA) {
-    // PPM along x2 with each slope and each raw interface value formed once
-    // for the block (para_dq, para_face) in shared memory after the tile:
-    // slopes at tile rows 1 .. BY+3 (every warp its own zone row, warps 0-2
-    // one more), raw values below tile rows 2 .. BY+3 (warps 0-1 one more),
-    // then every zone limits its own two (para_limit)
-    T* dq2 = reinterpret_cast<T*>(tile + NPR * PS);
-    T* fv2 = dq2 + NPR * (BY + 3) * 32;
-    const double* tc = tz - (ty + 3) * FLUX_TILE_W;  // the zone's column, tile row 0
-    auto dq_row = [&](int r) {
+  zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
 #pragma unroll
-      for (int k = 0; k < NPR; k++) {
-        const double* c = tc + k * PS + r * FLUX_TILE_W;
-        dq2[(k * (BY + 3) + r - 1) * 32 + tx] = para_dq((T)c[-FLUX_TILE_W], (T)c[0], (T)c[FLUX_TILE_W]);
-      }
-    };
-    dq_row(ty + 3);
-    if (ty < 2) dq_row(ty + 1);
-    else if (ty == 2) dq_row(BY + 3);
-    __syncthreads();
-    auto fv_row = [&](int r) {
+  for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
+  __syncthreads();
+  if (ty > 0) {
 #pragma unroll
-      for (int k = 0; k < NPR; k++) {
-        const double* c = tc + k * PS + r * FLUX_TILE_W;
-        const T* d = dq2 + (k * (BY + 3) + r - 1) * 32 + tx;
-        fv2[(k * (BY + 2) + r - 2) * 32 + tx] = para_face((T)c[-FLUX_TILE_W], (T)c[0], d[-32], d[0]);
-      }
-    };
-    fv_row(ty + 3);
-    if (ty == 0) fv_row(2);
-    else if (ty == 1) fv_row(BY + 3);
-    __syncthreads();
-    auto limit_row = [&](int r, T* Lo, T* Ro) {
-#pragma unroll
-      for (int k = 0; k < NPR; k++) {
-        const double* c = tc + k * PS + r * FLUX_TILE_W;
-        const T* f = fv2 + (k * (BY + 2) + r - 2) * 32 + tx;
-        para_limit((T)c[-FLUX_TILE_W], (T)c[0], (T)c[FLUX_TILE_W], f[0], f[32], Lo[k], Ro[k]);
-      }
-    };
-    limit_row(ty + 3, L, R);
-    // the slopes are read; their space takes the right states for the row above
-    T* shx = dq2;
-#pragma unroll
-    for (int k = 0; k < NPR; k++) shx[(k * BY + ty) * 32 + tx] = R[k];
-    __syncthreads();
-    if (ty > 0) {
-#pragma unroll
-      for (int k = 0; k < NPR; k++) pl[k] = shx[(k * BY + ty - 1) * 32 + tx];
-    } else {
-      T Lm[NPR];
-      limit_row(2, Lm, pl);
-    }
+    for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
   } else {
-    zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
-#pragma unroll
-    for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
-    __syncthreads();
-    if (ty > 0) {
-#pragma unroll
-      for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
-    } else {
-      T Lm[NPR];
-      zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
-    }
+    T Lm[NPR];
+    zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
   }
   if (in && j >= 0 && own) {
-    face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij);
+    face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij, rf);
     dt2 = (dtij < dt2) ? dtij : dt2;
     const bool polar = (j == 0 || j == n2) && (i < n1);
     const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
@@ -284,9 +259,7 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
 template <typename T, bool PARA, bool FFDE, int BY>
 inline void flux_launch_by(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, const CUtensorMap& map)
 {
-  // the tile, and for PPM the x2 slopes (BY + 3 rows) and raw interface
-  // values (BY + 2 rows) of 32 columns
-  constexpr size_t sm = flux_tile_bytes(BY) + (PARA ? (size_t)NPR * (2 * BY + 5) * 32 * sizeof(T) : 0);
+  constexpr size_t sm = flux_tile_bytes(BY);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_flux<T, PARA, FFDE, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -344,8 +317,12 @@ __global__ void k_emf(StepArgs a, const double* __restrict__ pv)
 
 // ---------------------------------------------------------------- update
 // Newton iterations a zone may take inside k_update before it is handed to
-// k_update_tail (the reference's limit is 200; typical zones need 2-4).
-constexpr int NEWTON_MAIN_CAP = 16;
+// k_update_tail, which continues the solve from the saved state (the
+// reference's limit is 200; typical zones need 2-4).
+#ifndef HARM_NEWTON_CAP
+#define HARM_NEWTON_CAP 16
+#endif
+constexpr int NEWTON_MAIN_CAP = HARM_NEWTON_CAP;
 
 // pflag store + fixup1zone (fixup.c:274-377: floors then the Lorentz factor
 // limit) + store of the new primitives; frho, fu: the zone's floors
@@ -372,7 +349,7 @@ __device__ __forceinline__ void finish_zone(const StepArgs& a, const Geo<double>
 // over the geometry block with the box above) while U(p_i) and the flux
 // divergence are formed from global loads; the block width is even.
 template <typename FT, bool FFDE>
-__global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const __grid_constant__ CUtensorMap geo_map,
+__global__ void __launch_bounds__(128, 4) k_update(StepArgs a, const __grid_constant__ CUtensorMap geo_map,
                                                 const double* __restrict__ pi, const double* __restrict__ pb,
                                                 double* __restrict__ pf, double c2)
 {
@@ -487,11 +464,14 @@ __global__ void __launch_bounds__(128, 3) k_update(StepArgs a, const __grid_cons
     return;
   }
   int niter;
-  int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP);
+  // a deferred solve leaves its Newton state in the repair scratch (idle
+  // until k_fixup_compute), NEWTON_STATE planes
+  int pfl = utoprim_2d(U, g, pfz, gam, a.pp.gammafail, &niter, NEWTON_MAIN_CAP, a.fixbuf + z, pl);
   if (pfl == NEWTON_DEFERRED || (a.pp.tryagain && pfl != 0)) {
     // rare slow inversion: hand the zone to k_update_tail so that this warp
     // is not held for up to 200 iterations by one lane (with the retry
-    // chain on, failed inversions go there too)
+    // chain on, failed inversions go there too, to be solved afresh)
+    if (pfl != NEWTON_DEFERRED) a.fixbuf[(NEWTON_STATE - 1) * pl + z] = -1.0;
 #pragma unroll
     for (int k = 0; k < NPR; k++) a.ubuf[k * pl + z] = U[k];
     a.worklist[atomicAdd(&a.sc->ndeferred, 1)] = (int)z;
@@ -532,9 +512,9 @@ inline void update_launch(dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, con
 // ---------------------------------------------------------------- end of step
 // diag_flux() for the global region's inner x1 face (diag.c:576-833): the
 // face fluxes in diagnostic form (UtoU UEVOLVE->UDIAG) and the energy-
-// equation stress terms 3 and 6 from the zone-centred state of row j.
+// equation stress terms 3 and 6 from the zone-centred state pr of row j.
 template <typename FT>
-__device__ __forceinline__ void horizon_terms(const StepArgs& a, const double* __restrict__ pv, int j, double* t4)
+__device__ __forceinline__ void horizon_terms(const StepArgs& a, const double* pr, int j, double* t4)
 {
   const FT* F1 = reinterpret_cast<const FT*>(a.F1);
   const long long pl = a.gr.plane;
@@ -547,9 +527,6 @@ __device__ __forceinline__ void horizon_terms(const StepArgs& a, const double* _
   gu += -gr;
   t4[0] = gr * gf;
   t4[1] = gu * gf;
-  double pr[NPR];
-#pragma unroll
-  for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
   Geo<double> g;
   load_geo(a, CENT, z, g);
   State<double> q;
@@ -562,35 +539,50 @@ __device__ __forceinline__ void horizon_terms(const StepArgs& a, const double* _
   t4[3] = -(q.bcon[1]) * (q.bcov[0]) * surgdet;
 }
 
-// After the last substep, one block: the horizon terms of every row j, their
-// sums in j order as the reference's loop adds them (so the sums are exact),
-// pcum += pdot * dt (diag.c:576-833); then the new dt from the flux blocks'
-// Courant minima (advance.c:190, step_ch.c:174-183) and t += dt.
-constexpr int STEP_END_THREADS = 1024;
-template <typename FT>
-__global__ void __launch_bounds__(STEP_END_THREADS) k_step_end(StepArgs a, const double* __restrict__ pv)
+// The end of a step, by every thread of one block, after the horizon terms
+// of every row j sit in t[k * ts + j] (k < 4): their sums in j order as the
+// reference's loop adds them (so the sums are exact), pcum += pdot * dt
+// (diag.c:576-833); then the new dt from the flux blocks' Courant minima
+// (advance.c:190, step_ch.c:174-183) and t += dt.  L2: the terms were
+// written by other blocks of the same kernel (read past L1).
+template <bool L2>
+__device__ __forceinline__ void step_end_finish(const StepArgs& a, const double* t, long long ts)
 {
+  constexpr int CHUNK = 256;
   __shared__ double sh[2][32];
   __shared__ double acc[4];
-  __shared__ double buf[4][STEP_END_THREADS];
-  if (threadIdx.x < 4) acc[threadIdx.x] = 0.;
-  for (int j0 = 0; j0 < a.gr.n2; j0 += STEP_END_THREADS) {
-    const int m = (a.gr.n2 - j0 < STEP_END_THREADS) ? a.gr.n2 - j0 : STEP_END_THREADS;
-    if ((int)threadIdx.x < m) {
-      double t4[4];
-      horizon_terms<FT>(a, pv, j0 + threadIdx.x, t4);
-#pragma unroll
-      for (int k = 0; k < 4; k++) buf[k][threadIdx.x] = t4[k];
+  __shared__ double stage[4][CHUNK];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+  const int n2 = a.gr.n2;
+  // chunks of the four term rows are staged in shared memory by the whole
+  // block (independent loads), then four threads add them one after another
+  // in j order
+  double s = 0.;
+  for (int j0 = 0; j0 < n2; j0 += CHUNK) {
+    const int m = (n2 - j0 < CHUNK) ? n2 - j0 : CHUNK;
+    for (int q = tid; q < 4 * m; q += nt) {
+      const int k = q / m, jj = q - k * m;
+      const double* src = t + k * ts + j0 + jj;
+      stage[k][jj] = L2 ? __ldcg(src) : *src;
     }
     __syncthreads();
-    if (threadIdx.x < 4) {
-      double s = acc[threadIdx.x];
-      for (int q = 0; q < m; q++) s += buf[threadIdx.x][q];
-      acc[threadIdx.x] = s;
+    if (tid < 4) {
+      const double* b = stage[tid];
+      int q = 0;
+      for (; q + 8 <= m; q += 8) {
+        double v[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) v[r] = b[q + r];
+#pragma unroll
+        for (int r = 0; r < 8; r++) s += v[r];
+      }
+      for (; q < m; q++) s += b[q];
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
+  if (tid < 4) acc[tid] = s;
+  __syncthreads();
+  if (tid == 0) {
     DevScalars* sc = a.sc;
     for (int k = 0; k < 4; k++) sc->hz[k] = acc[k];
     sc->hz[4] += acc[0] * sc->dt;
@@ -598,14 +590,15 @@ __global__ void __launch_bounds__(STEP_END_THREADS) k_step_end(StepArgs a, const
     sc->hz[6] += (acc[2] + acc[3]) * sc->dt;
   }
   double m1 = 1.e9, m2 = 1.e9;
-  for (int b = threadIdx.x; b < a.nblocks_flux; b += blockDim.x) {
-    double v1 = a.blockmin[b], v2 = a.blockmin[a.nblocks_flux + b];
+#pragma unroll 4
+  for (int b = tid; b < a.nblocks_flux; b += nt) {
+    double v1 = __ldcg(a.blockmin + b), v2 = __ldcg(a.blockmin + a.nblocks_flux + b);
     m1 = (v1 < m1) ? v1 : m1;
     m2 = (v2 < m2) ? v2 : m2;
   }
   m1 = block_min(m1, sh[0]);
   m2 = block_min(m2, sh[1]);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     DevScalars* s = a.sc;
     double ndt = a.pp.defcon * 1. / (1. / m1 + 1. / m2);
     s->ndt = ndt;
@@ -617,6 +610,26 @@ __global__ void __launch_bounds__(STEP_END_THREADS) k_step_end(StepArgs a, const
     if (moved) s->dt_free = ndt;  // a step at dt = 0 (past the end time) keeps the last one
     if (s->t + s->dt > a.pp.tf) s->dt = a.pp.tf - s->t;
   }
+}
+
+// After the last substep, one block: the horizon terms of every row j (into
+// the inversion scratch ubuf, idle by now), then step_end_finish.
+constexpr int STEP_END_THREADS = 512;
+template <typename FT>
+__global__ void __launch_bounds__(STEP_END_THREADS) k_step_end(StepArgs a, const double* __restrict__ pv)
+{
+  const long long pl = a.gr.plane;
+  for (int j = threadIdx.x; j < a.gr.n2; j += blockDim.x) {
+    const long long z = a.gr.at(0, j);
+    double pr[NPR], t4[4];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * pl + z];
+    horizon_terms<FT>(a, pr, j, t4);
+#pragma unroll
+    for (int k = 0; k < 4; k++) a.ubuf[k * pl + j] = t4[k];
+  }
+  __syncthreads();
+  step_end_finish<false>(a, a.ubuf, pl);
 }
 
 }  // namespace harm

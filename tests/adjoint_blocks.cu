@@ -1,8 +1,12 @@
-// Test harness (host code): each adjoint building block of
+// Test harness: each adjoint building block of
 // harm_ramt_b200/csrc/harm_adjoint.cuh against central finite differences
-// of its forward function, on given states and geometry.  Built with nvcc by
-// tests/test_adjoint_blocks.py; every check returns the relative error
+// of its forward function, on given states and geometry (host code), and the
+// update adjoint's two blocks run on the device as one kernel and as two,
+// against their host build (tests/test_gpu_adjoint_blocks.py).  Built with
+// nvcc (host, and sm_100a device code) by tests/test_adjoint_blocks.py; every
+// check returns the relative error
 // |lambda . dF/dp v (finite difference) - pbar . v| / max(|.|, |.|).
+#include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
 
@@ -12,7 +16,7 @@ using namespace harm;
 
 namespace {
 
-Geo<double> geo_of(const double* gcov16, const double* gcon16, double gdet)
+__host__ __device__ Geo<double> geo_of(const double* gcov16, const double* gcon16, double gdet)
 {
   Geo<double> g;
   for (int a = 0; a < 4; a++)
@@ -290,6 +294,120 @@ void ab_source(const double* p, const double* gcov16, const double* gcon16, doub
     lam[l] = 1.;
     out4[l] = source_value(p, g, gam, conn40, lam);
   }
+}
+
+}  // extern "C"
+
+// ---- the update adjoint's two blocks in one kernel and in two, on the device
+// and on the host: x = ift_solve(p1, b) (the con-to-prim step), then the
+// geometric source's adjoint at pb with dUg's adjoint c dt x[UU..U3].  The
+// arrays hold n zones: p1, pb, b 8 a zone, geo 16 + 16 + 1 (gcov, gcon,
+// gdet), conn 64 (Gamma^k_lj, k-major); outputs x and lb 8 a zone (x = 0
+// where the solve reports a singular matrix).
+
+namespace {
+
+__host__ __device__ void probe_ift(const double* p1, const double* b, const double* geo, double gam, double* x)
+{
+  const Geo<double> g = geo_of(geo, geo + 16, geo[32]);
+  if (ift_solve(p1, g, gam, b, x))
+    for (int k = 0; k < NPR; k++) x[k] = 0.;
+}
+
+__host__ __device__ void probe_source(const double* pb, const double* x, const double* geo, const double* conn64,
+                                      double gam, double cdt, double* lb)
+{
+  const Geo<double> g = geo_of(geo, geo + 16, geo[32]);
+  double conn40[40];
+  for (int k = 0; k < 4; k++)
+    for (int l = 0; l < 4; l++)
+      for (int j = l; j < 4; j++) conn40[k * 10 + sym(l, j)] = conn64[(k * 4 + l) * 4 + j];
+  double dUgb[4];
+  for (int l = 0; l < 4; l++) dUgb[l] = cdt * x[UU + l];
+  for (int k = 0; k < NPR; k++) lb[k] = 0.;
+  adj_source(pb, g, gam, conn40, dUgb, lb);
+}
+
+__global__ void k_probe_fused(int n, const double* p1, const double* pb, const double* b, const double* geo,
+                              const double* conn, double gam, double cdt, double* x, double* lb)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  double xz[NPR], lz[NPR];
+  probe_ift(p1 + 8 * z, b + 8 * z, geo + 33 * z, gam, xz);
+  probe_source(pb + 8 * z, xz, geo + 33 * z, conn + 64 * z, gam, cdt, lz);
+  for (int k = 0; k < NPR; k++) {
+    x[8 * z + k] = xz[k];
+    lb[8 * z + k] = lz[k];
+  }
+}
+
+__global__ void k_probe_ift(int n, const double* p1, const double* b, const double* geo, double gam, double* x)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z < n) probe_ift(p1 + 8 * z, b + 8 * z, geo + 33 * z, gam, x + 8 * z);
+}
+
+__global__ void k_probe_source(int n, const double* pb, const double* x, const double* geo, const double* conn,
+                               double gam, double cdt, double* lb)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z < n) probe_source(pb + 8 * z, x + 8 * z, geo + 33 * z, conn + 64 * z, gam, cdt, lb + 8 * z);
+}
+
+}  // namespace
+
+extern "C" {
+
+void ab_probe_host(int n, const double* p1, const double* pb, const double* b, const double* geo, const double* conn,
+                   double gam, double cdt, double* x, double* lb)
+{
+  for (int z = 0; z < n; z++) {
+    probe_ift(p1 + 8 * z, b + 8 * z, geo + 33 * z, gam, x + 8 * z);
+    probe_source(pb + 8 * z, x + 8 * z, geo + 33 * z, conn + 64 * z, gam, cdt, lb + 8 * z);
+  }
+}
+
+// fused = 1: one kernel (k_probe_fused), 0: two (k_probe_ift, k_probe_source).
+// Returns 0, or the CUDA error code.
+int ab_probe_device(int fused, int n, const double* p1, const double* pb, const double* b, const double* geo,
+                    const double* conn, double gam, double cdt, double* x, double* lb)
+{
+  const size_t s8 = sizeof(double) * 8 * n, sg = sizeof(double) * 33 * n, sc = sizeof(double) * 64 * n;
+  double *dp1 = nullptr, *dpb = nullptr, *db = nullptr, *dg = nullptr, *dc = nullptr, *dx = nullptr, *dl = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMalloc(&dp1, s8);
+  if (e == cudaSuccess) e = cudaMalloc(&dpb, s8);
+  if (e == cudaSuccess) e = cudaMalloc(&db, s8);
+  if (e == cudaSuccess) e = cudaMalloc(&dg, sg);
+  if (e == cudaSuccess) e = cudaMalloc(&dc, sc);
+  if (e == cudaSuccess) e = cudaMalloc(&dx, s8);
+  if (e == cudaSuccess) e = cudaMalloc(&dl, s8);
+  if (e == cudaSuccess) e = cudaMemcpy(dp1, p1, s8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dpb, pb, s8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(db, b, s8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dg, geo, sg, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dc, conn, sc, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const int th = 128, bl = (n + th - 1) / th;
+    if (fused) {
+      k_probe_fused<<<bl, th>>>(n, dp1, dpb, db, dg, dc, gam, cdt, dx, dl);
+    } else {
+      k_probe_ift<<<bl, th>>>(n, dp1, db, dg, gam, dx);
+      k_probe_source<<<bl, th>>>(n, dpb, dx, dg, dc, gam, cdt, dl);
+    }
+    e = cudaDeviceSynchronize();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(x, dx, s8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(lb, dl, s8, cudaMemcpyDeviceToHost);
+  cudaFree(dp1);
+  cudaFree(dpb);
+  cudaFree(db);
+  cudaFree(dg);
+  cudaFree(dc);
+  cudaFree(dx);
+  cudaFree(dl);
+  return (int)e;
 }
 
 }  // extern "C"

@@ -26,8 +26,8 @@ def _lib():
     deps = [SRC] + HDRS
     if not os.path.exists(LIB) or any(os.path.getmtime(d) > os.path.getmtime(LIB) for d in deps):
         os.makedirs(os.path.dirname(LIB), exist_ok=True)
-        subprocess.run([nvcc, "-O2", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-o",
-                        LIB + ".tmp", SRC], check=True)
+        subprocess.run([nvcc, "-O2", "--fmad=false", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-Xcompiler", "-fPIC", "-shared", "-o", LIB + ".tmp", SRC], check=True)
         os.replace(LIB + ".tmp", LIB)
     lib = ctypes.CDLL(LIB)
     d, i = ctypes.c_double, ctypes.c_int
@@ -42,6 +42,9 @@ def _lib():
     lib.ab_check_source.argtypes = [P, P, P, P, P, d, P, d, d]
     lib.ab_check_ift.restype = d
     lib.ab_check_ift.argtypes = [P, P, P, P, P, d, d, d]
+    lib.ab_probe_host.argtypes = [i, P, P, P, P, P, d, d, P, P]
+    lib.ab_probe_device.restype = i
+    lib.ab_probe_device.argtypes = [i, i, P, P, P, P, P, d, d, P, P]
     return lib
 
 
