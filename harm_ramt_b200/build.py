@@ -19,8 +19,11 @@ HEADERS = ["harm_device.cuh", "harm_kernels.cuh", "harm_step_impl.cuh", "harm_ad
 COMMON = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 # FP64 path: no contraction, IEEE division/square root (bit parity with the reference)
 EXACT = ["--fmad=false"]
-# mixed-precision instantiations only: contraction and fast FP32 division/sqrt
-FAST = ["--fmad=true", "--prec-div=false", "--prec-sqrt=false", "--ftz=true"]
+# mixed-precision instantiations only: contraction and fast FP32 division/sqrt.
+# FP32 denormals are kept: with flush-to-zero added, the mixed form's distance
+# from FP64 on the 64^2 torus at t = 20 grew from 2.3e-6 to 3.1e-4 (rho L1),
+# while any two of the three fast options alone stayed at 2-3e-6.
+FAST = ["--fmad=true", "--prec-div=false", "--prec-sqrt=false", "--ftz=false"]
 FLAGS = {"harm_step_mixed.cu": FAST}
 NVCC_FLAGS = COMMON + EXACT  # kept for reference by tools that print the build line
 

@@ -173,16 +173,19 @@ __device__ __forceinline__ double gdet_at(const StepArgs& a, int loc, long long 
   return __ldg(a.geo + ((long long)loc * GEO_PER_LOC + 20) * a.gr.plane + z);
 }
 
-// k_flux blocks: 32 zones along x1 (one warp) x 4 or 16 rows.  Neighbouring
+// k_flux blocks: 32 zones along x1 (one warp) x 4 or 8 rows.  Neighbouring
 // blocks overlap by one zone along x1, so that each covers FLUX_BX x1 faces
-// without recomputing a neighbour's interface state.  16 rows leave less
-// x2 recomputation (one row in 16) but hold one 512-thread block per SM:
-// they are used when that grid still fills three waves of the 148 SMs,
-// 4 rows (four 128-thread blocks per SM) on smaller grids.  The FP32 faces
-// of the mixed form fit 128 registers without spilling and run best as
-// 4-row blocks at four per SM on any grid.
+// without recomputing a neighbour's interface state.  8 rows (two 256-thread
+// blocks per SM at 128 registers: one block's tile copy overlaps the other's
+// faces) are used when that grid still fills three waves of the 148 SMs, 4
+// rows (four 128-thread blocks per SM) on smaller grids.  Measured on the
+// developed 512^2 torus (step time, three runs each): 8 rows 0.5373-0.5405
+// ms, 16 rows (one 512-thread block per SM) 0.5427-0.5463, 15 rows (one
+// block per SM, 4.0 waves) 0.5770-0.5799.  The FP32 faces of the mixed form
+// fit 128 registers without spilling and run best as 4-row blocks at four
+// per SM on any grid.
 #ifndef HARM_FLUX_BY_LARGE
-#define HARM_FLUX_BY_LARGE 16
+#define HARM_FLUX_BY_LARGE 8
 #endif
 constexpr int FLUX_BX = 31, FLUX_BY_SMALL = 4, FLUX_BY_LARGE = HARM_FLUX_BY_LARGE;
 // k_flux's primitive tile (one TMA box over a state's 8 planes): the 32

@@ -139,7 +139,7 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // (blocks step by FLUX_BX = 31 along x1): lane 0 only lends its right state,
 // and its faces are the previous block's (block 0's lane 0 is zone -1,
 // which has no x1 face but an x2 face).
-// BY = 4 or 16 rows per block (flux_rows).  At most 128 registers a thread:
+// BY = 4 or 8 rows per block (flux_rows).  At most 128 registers a thread:
 // 512 threads per SM for the FP64 faces, four 4-row blocks for the FP32 ones.
 template <typename T, bool PARA, bool FFDE, int BY>
 __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 4 : 1))

@@ -328,6 +328,74 @@ __host__ __device__ void probe_source(const double* pb, const double* x, const d
   adj_source(pb, g, gam, conn40, dUgb, lb);
 }
 
+// The con-to-prim step as the first build of the update adjoint formed it:
+// the full 8 x 8 Jacobian (one reverse sweep per row) in a local array and
+// Gaussian elimination with partial pivoting on its transpose, also local.
+// In that build the source adjoint computed after it in the same kernel
+// differed from the host's; the mode that runs it here shows whether that
+// configuration still does.
+__host__ __device__ int legacy_ift(const double* p, const double* geo, double gam, const double* b, double* x)
+{
+  const Geo<double> g = geo_of(geo, geo + 16, geo[32]);
+  double J[NPR][NPR];
+  {
+    State<double> q;
+    state_of(p, g, q);
+    for (int r = 0; r < NPR; r++) {
+      double Fb[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+      Fb[r] = 1.;
+      StateAdj qb;
+      qb.zero();
+      double row[NPR] = {0., 0., 0., 0., 0., 0., 0., 0.};
+      adj_flux(p, q, 0, g, gam, Fb, qb, row);
+      adj_state(p, g, q, qb, row);
+      for (int c = 0; c < NPR; c++) J[r][c] = row[c];
+    }
+  }
+  double A[NPR][NPR + 1];
+  for (int r = 0; r < NPR; r++) {
+    for (int c = 0; c < NPR; c++) A[r][c] = J[c][r];
+    A[r][NPR] = b[r];
+  }
+  for (int col = 0; col < NPR; col++) {
+    int piv = col;
+    for (int r = col + 1; r < NPR; r++)
+      if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
+    if (A[piv][col] == 0.0) return 1;
+    if (piv != col)
+      for (int c = 0; c <= NPR; c++) {
+        const double t = A[col][c];
+        A[col][c] = A[piv][c];
+        A[piv][c] = t;
+      }
+    for (int r = col + 1; r < NPR; r++) {
+      const double f = A[r][col] / A[col][col];
+      for (int c = col; c <= NPR; c++) A[r][c] -= f * A[col][c];
+    }
+  }
+  for (int r = NPR - 1; r >= 0; r--) {
+    double s = A[r][NPR];
+    for (int c = r + 1; c < NPR; c++) s -= A[r][c] * x[c];
+    x[r] = s / A[r][r];
+  }
+  return 0;
+}
+
+__global__ void k_probe_legacy(int n, const double* p1, const double* pb, const double* b, const double* geo,
+                               const double* conn, double gam, double cdt, double* x, double* lb)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  double xz[NPR], lz[NPR];
+  if (legacy_ift(p1 + 8 * z, geo + 33 * z, gam, b + 8 * z, xz))
+    for (int k = 0; k < NPR; k++) xz[k] = 0.;
+  probe_source(pb + 8 * z, xz, geo + 33 * z, conn + 64 * z, gam, cdt, lz);
+  for (int k = 0; k < NPR; k++) {
+    x[8 * z + k] = xz[k];
+    lb[8 * z + k] = lz[k];
+  }
+}
+
 __global__ void k_probe_fused(int n, const double* p1, const double* pb, const double* b, const double* geo,
                               const double* conn, double gam, double cdt, double* x, double* lb)
 {
@@ -359,16 +427,23 @@ __global__ void k_probe_source(int n, const double* pb, const double* x, const d
 
 extern "C" {
 
-void ab_probe_host(int n, const double* p1, const double* pb, const double* b, const double* geo, const double* conn,
-                   double gam, double cdt, double* x, double* lb)
+// legacy = 1: the con-to-prim step of legacy_ift
+void ab_probe_host(int legacy, int n, const double* p1, const double* pb, const double* b, const double* geo,
+                   const double* conn, double gam, double cdt, double* x, double* lb)
 {
   for (int z = 0; z < n; z++) {
-    probe_ift(p1 + 8 * z, b + 8 * z, geo + 33 * z, gam, x + 8 * z);
+    if (legacy) {
+      if (legacy_ift(p1 + 8 * z, geo + 33 * z, gam, b + 8 * z, x + 8 * z))
+        for (int k = 0; k < NPR; k++) x[8 * z + k] = 0.;
+    } else {
+      probe_ift(p1 + 8 * z, b + 8 * z, geo + 33 * z, gam, x + 8 * z);
+    }
     probe_source(pb + 8 * z, x + 8 * z, geo + 33 * z, conn + 64 * z, gam, cdt, lb + 8 * z);
   }
 }
 
-// fused = 1: one kernel (k_probe_fused), 0: two (k_probe_ift, k_probe_source).
+// fused = 1: one kernel (k_probe_fused), 0: two (k_probe_ift, k_probe_source),
+// 2: one kernel with the legacy con-to-prim step (k_probe_legacy).
 // Returns 0, or the CUDA error code.
 int ab_probe_device(int fused, int n, const double* p1, const double* pb, const double* b, const double* geo,
                     const double* conn, double gam, double cdt, double* x, double* lb)
@@ -390,7 +465,9 @@ int ab_probe_device(int fused, int n, const double* p1, const double* pb, const 
   if (e == cudaSuccess) e = cudaMemcpy(dc, conn, sc, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     const int th = 128, bl = (n + th - 1) / th;
-    if (fused) {
+    if (fused == 2) {
+      k_probe_legacy<<<bl, th>>>(n, dp1, dpb, db, dg, dc, gam, cdt, dx, dl);
+    } else if (fused) {
       k_probe_fused<<<bl, th>>>(n, dp1, dpb, db, dg, dc, gam, cdt, dx, dl);
     } else {
       k_probe_ift<<<bl, th>>>(n, dp1, db, dg, gam, dx);

@@ -42,7 +42,7 @@ def _lib():
     lib.ab_check_source.argtypes = [P, P, P, P, P, d, P, d, d]
     lib.ab_check_ift.restype = d
     lib.ab_check_ift.argtypes = [P, P, P, P, P, d, d, d]
-    lib.ab_probe_host.argtypes = [i, P, P, P, P, P, d, d, P, P]
+    lib.ab_probe_host.argtypes = [i, i, P, P, P, P, P, d, d, P, P]
     lib.ab_probe_device.restype = i
     lib.ab_probe_device.argtypes = [i, i, P, P, P, P, P, d, d, P, P]
     return lib

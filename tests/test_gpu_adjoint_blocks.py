@@ -48,7 +48,7 @@ def test_update_adjoint_blocks_fused_and_split_equal_host(harm):
     nz, p1, pb, b, geo, conn, gam, cdt = _inputs(harm)
     ins = [_p(x) for x in (p1, pb, b, geo, conn)]
     xh, lh = np.zeros((nz, 8)), np.zeros((nz, 8))
-    lib.ab_probe_host(nz, *[q for _, q in ins], gam, cdt, _p(xh)[1], _p(lh)[1])
+    lib.ab_probe_host(0, nz, *[q for _, q in ins], gam, cdt, _p(xh)[1], _p(lh)[1])
     assert np.isfinite(lh).all() and np.count_nonzero(xh) > 0
     for fused in (1, 0):
         xd, ld = np.zeros((nz, 8)), np.zeros((nz, 8))
@@ -59,3 +59,14 @@ def test_update_adjoint_blocks_fused_and_split_equal_host(harm):
         assert np.array_equal(ld, lh), (f"{what}: source adjoint differs in {np.count_nonzero(ld != lh)} values, "
                                         f"max rel {np.max(np.abs(ld - lh) / np.maximum(np.abs(lh), 1e-300)):.3e}")
     print(f"\nupdate adjoint blocks, {nz} zones: device (one kernel and two) == host, bit for bit")
+    # the first build's con-to-prim step (8 x 8 local arrays) with the source
+    # adjoint in the same kernel: reported against its own host build
+    xl, ll = np.zeros((nz, 8)), np.zeros((nz, 8))
+    lib.ab_probe_host(1, nz, *[q for _, q in ins], gam, cdt, _p(xl)[1], _p(ll)[1])
+    xd, ld = np.zeros((nz, 8)), np.zeros((nz, 8))
+    assert lib.ab_probe_device(2, nz, *[q for _, q in ins], gam, cdt, _p(xd)[1], _p(ld)[1]) == 0
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+    print(f"legacy 8x8 solve + source adjoint in one kernel: solve differs from the host in "
+          f"{np.count_nonzero(xd != xl)} values (max rel {rel(xd, xl):.2e}), source adjoint in "
+          f"{np.count_nonzero(ld != ll)} (max rel {rel(ld, ll):.2e}); legacy vs current solve on the host: "
+          f"max rel {rel(xl, xh):.2e}")
