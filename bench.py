@@ -365,14 +365,15 @@ def b200_arm(a):
     dom = max(prof, key=lambda k: prof[k][0])
     dom_ms, dom_launches = prof[dom]
     per_launch_ms = dom_ms / max(dom_launches, 1)
-    alg_bytes = KERNEL_BYTES.get(dom, 0) * n * n
+    kbytes = {**KERNEL_BYTES, **(KERNEL_BYTES_SWITCH if a.fluxadjust else {})}
+    alg_bytes = kbytes.get(dom, 0) * n * n
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
     step_alg = BYTES_PER_ZONE_CYCLE * n * n / (ms_step * 1e-3) / 1e9
     total_prof = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": (TRAFFIC_512[dom] * (n * n) / (512 * 512)) if dom in TRAFFIC_512 else None,
-                "bytes_per_zone": KERNEL_BYTES.get(dom, 0), "launch_ms": per_launch_ms,
+                "bytes_per_zone": kbytes.get(dom, 0), "launch_ms": per_launch_ms,
                 "share_of_step": dom_ms / total_prof if total_prof else None,
                 "whole_step": {"achieved": step_alg, "frac": step_alg / peak,
                                "bytes_per_zone_cycle": BYTES_PER_ZONE_CYCLE},
@@ -789,14 +790,19 @@ KERNEL_BYTES = {
     "k_emf": 8 * (2 + 3 + 1),
     "k_bsqflags": 8 * (8 + 21) + 1,
 }
-# FP64 instructions (thread level, every FP64-pipe instruction: adds,
-# multiplies, the FMAs and comparisons of division and square root) per
-# active zone of one launch, from one ncu capture of each kernel at 512^2
-# (sm__inst_executed_pipe_fp64.sum x 32 / zones; profiles/)
-FP64_INSTR_PER_ZONE = {}
-# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
-# at 512^2 (profiles/k_*_torus512_fp64_para_hll.md), scaled by zone count
-TRAFFIC_512 = {"k_flux": 113.8e6, "k_update": 212.2e6}
+# with the per-zone HLL/LAXF switch the first substep's k_flux also reads the
+# CENT geometry (21 values) and writes the two flag bytes, the second reads
+# the flux choice: averaged over the two launches of a step
+KERNEL_BYTES_SWITCH = {"k_flux": KERNEL_BYTES["k_flux"] + (8 * 21 + 2 + 1) / 2}
+# FP64-pipe instructions (thread slots: adds, multiplies, comparisons and the
+# FMAs of division and square root) per active zone of one launch, from one
+# ncu capture of each kernel at 512^2 in the developed flow
+# (sm__inst_executed_pipe_fp64.sum x 32 / zones; profiles/k_flux_*, k_update_*;
+# the k_flux launch captured is a first substep, which also forms the flags)
+FP64_INSTR_PER_ZONE = {"k_flux": 3940, "k_update": 1983}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from the same
+# captures, scaled by zone count
+TRAFFIC_512 = {"k_flux": 145.9e6, "k_update": 196.6e6}
 
 
 def main():

@@ -972,13 +972,17 @@ int harm_ensemble_sync(harm_ensemble* e, harm_status* st)
 // ---------------------------------------------------------------- adjoint
 namespace {
 
+// The reverse pass keeps two record sets: while the adjoint of one
+// checkpoint segment runs from one set (on its own stream), the replay of
+// the segment before it records into the other (on the context's stream).
 struct AdjWork {
   std::vector<void*> mem;
-  std::vector<Rec> rec;        // one per step of a checkpoint segment
-  std::vector<double*> pnext;  // the state after each slot's step (the next slot's pn; an extra one at the end)
-  std::vector<cudaGraphExec_t> recg;  // the recording step of each slot, captured
-  std::vector<cudaGraphExec_t> adjg;  // the adjoint step of each slot, captured
+  std::vector<Rec> rec[2];        // one per step of a checkpoint segment, per set
+  std::vector<double*> pnext[2];  // the state after each slot's step (the next slot's pn; an extra one at the end)
+  std::vector<cudaGraphExec_t> recg[2];  // the recording step of each slot, captured
+  std::vector<cudaGraphExec_t> adjg[2];  // the adjoint step of each slot, captured
   double *La, *Lc, *Lb, *Lsnap, *LdU, *Le, *Sr, *dts, *dot;
+  DevScalars* sc_adj;  // the adjoint stream's scalars (its steps' dt), apart from the replay's
   bool ok = true;
   void* get(size_t bytes)
   {
@@ -992,10 +996,12 @@ struct AdjWork {
   }
   ~AdjWork()
   {
-    for (cudaGraphExec_t g : recg)
-      if (g) cudaGraphExecDestroy(g);
-    for (cudaGraphExec_t g : adjg)
-      if (g) cudaGraphExecDestroy(g);
+    for (int x = 0; x < 2; x++) {
+      for (cudaGraphExec_t g : recg[x])
+        if (g) cudaGraphExecDestroy(g);
+      for (cudaGraphExec_t g : adjg[x])
+        if (g) cudaGraphExecDestroy(g);
+    }
     for (void* p : mem) cudaFree(p);
   }
 };
@@ -1014,26 +1020,31 @@ size_t dot_blocks(const harm_ctx* c)
 }
 
 // nslots: steps per checkpoint segment.  Each keeps its own record, about
-// 10 state-sized arrays: a 16-step segment of a 512^2 grid holds ~3 GB.
-int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps, int nslots)
+// 10 state-sized arrays, in each of the two sets: a 16-step segment of a
+// 512^2 grid holds ~3 GB per set.  nsets: 2 when there is more than one
+// segment (replay and adjoint overlap), else 1.
+int adj_alloc(harm_ctx* c, AdjWork& w, int nsteps, int nslots, int nsets)
 {
   const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
-  w.rec.resize(nslots);
-  for (Rec& r : w.rec) {
-    r.pn = (double*)w.get(P);
-    r.ph = (double*)w.get(P);
-    for (int s = 0; s < 2; s++) {
-      r.pinv[s] = (double*)w.get(P);
-      r.upd[s] = (double*)w.get(P);
-      r.snap[s] = (double*)w.get(P);
-      r.pre2[s] = (double*)w.get(P);
-      r.flaginv[s] = (int*)w.get(pl * sizeof(int));
-      r.flag[s] = (int*)w.get(pl * sizeof(int));
-      r.fixset[s] = (unsigned char*)w.get(pl);
+  for (int x = 0; x < nsets; x++) {
+    w.rec[x].resize(nslots);
+    for (Rec& r : w.rec[x]) {
+      r.pn = (double*)w.get(P);
+      r.ph = (double*)w.get(P);
+      for (int s = 0; s < 2; s++) {
+        r.pinv[s] = (double*)w.get(P);
+        r.upd[s] = (double*)w.get(P);
+        r.snap[s] = (double*)w.get(P);
+        r.pre2[s] = (double*)w.get(P);
+        r.flaginv[s] = (int*)w.get(pl * sizeof(int));
+        r.flag[s] = (int*)w.get(pl * sizeof(int));
+        r.fixset[s] = (unsigned char*)w.get(pl);
+      }
     }
+    double* plast = (double*)w.get(P);
+    for (int m = 0; m < nslots; m++) w.pnext[x].push_back(m + 1 < nslots ? w.rec[x][m + 1].pn : plast);
   }
-  double* plast = (double*)w.get(P);
-  for (int m = 0; m < nslots; m++) w.pnext.push_back(m + 1 < nslots ? w.rec[m + 1].pn : plast);
+  w.sc_adj = (DevScalars*)w.get(sizeof(DevScalars));
   w.La = (double*)w.get(P);
   w.Lc = (double*)w.get(P);
   w.Lb = (double*)w.get(P);
@@ -1221,10 +1232,11 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   if (!c->geo_ok) return HARM_EGEOMETRY;
   if (!adjoint_supported(c)) return HARM_EINVAL;
   AdjWork w;
-  int rc = adj_alloc(c, w, nsteps, std::min(checkpoint_every, nsteps));
+  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  const int nsets = (nck > 1) ? 2 : 1;
+  int rc = adj_alloc(c, w, nsteps, std::min(checkpoint_every, nsteps), nsets);
   if (rc) return rc;
   const size_t pl = (size_t)c->gr.plane, P = NPR * pl * sizeof(double);
-  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
   std::vector<Saved> ck(nck);
   for (auto& x : ck) x = Saved{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
   Saved fin{(double*)w.get(P), (double*)w.get(pl * sizeof(double))};
@@ -1261,44 +1273,97 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   save_state(c, fin);
   // reverse, segment by segment: recompute the segment from its checkpoint,
   // recording every step, then the steps' adjoints in reverse order (both
-  // as per-slot graphs, captured on first use)
-  w.recg.assign(w.rec.size(), nullptr);
-  w.adjg.assign(w.rec.size(), nullptr);
-  for (int sg = nck - 1; sg >= 0; sg--) {
-    const int n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
+  // as per-slot graphs, captured on first use).  The replay of segment sg-1
+  // (this context's stream, record set (sg-1) & 1) runs while the adjoint of
+  // segment sg (stream sa, set sg & 1) does: they share only the geometry
+  // (read) -- the adjoint's steps read their dt from their own scalars.  A
+  // set is replayed into only after the adjoint that read it has finished.
+  cudaStream_t sa = nullptr;
+  cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_adj[2] = {nullptr, nullptr}, ev_join = nullptr;
+  auto cleanup = [&]() {
+    for (int x = 0; x < 2; x++) {
+      if (ev_rec[x]) cudaEventDestroy(ev_rec[x]);
+      if (ev_adj[x]) cudaEventDestroy(ev_adj[x]);
+    }
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (sa) cudaStreamDestroy(sa);
+  };
+  CK(cudaStreamCreateWithFlags(&sa, cudaStreamNonBlocking));
+  for (int x = 0; x < 2; x++) {
+    CK(cudaEventCreateWithFlags(&ev_rec[x], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_adj[x], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  // the adjoint's context view: its own stream and scalars (a copy of the
+  // run's, whose dt each adjoint step sets)
+  harm_ctx ca = *c;
+  ca.stream = sa;
+  ca.d_sc = w.sc_adj;
+  const StepArgs aa = ca.args();
+  CK(cudaMemcpyAsync(w.sc_adj, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, s));
+  for (int x = 0; x < nsets; x++) {
+    w.recg[x].assign(w.rec[x].size(), nullptr);
+    w.adjg[x].assign(w.rec[x].size(), nullptr);
+  }
+  auto replay = [&](int sg) -> int {
+    const int x = sg & (nsets - 1), n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
     load_state(c, ck[sg]);
     for (int m = 0; m < len; m++) {
-      if (!w.recg[m]) {
-        const Rec* r = &w.rec[m];
-        rc = capture_graph(c, [r](harm_ctx* t) { return enqueue_step(t, nullptr, r); }, &w.recg[m]);
-        if (rc != HARM_OK) return rc;
+      if (!w.recg[x][m]) {
+        const Rec* r = &w.rec[x][m];
+        const int rc2 = capture_graph(c, [r](harm_ctx* t) { return enqueue_step(t, nullptr, r); }, &w.recg[x][m]);
+        if (rc2 != HARM_OK) return rc2;
       }
       k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
-      CK(cudaGraphLaunch(w.recg[m], s));
+      CK(cudaGraphLaunch(w.recg[x][m], s));
     }
     // the segment's last state, where its last step's adjoint reads it
-    CK(cudaMemcpyAsync(w.pnext[len - 1], c->d_p, P, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(w.pnext[x][len - 1], c->d_p, P, cudaMemcpyDeviceToDevice, s));
+    CK(cudaEventRecord(ev_rec[x], s));
+    return HARM_OK;
+  };
+  if ((rc = replay(nck - 1)) != HARM_OK) {
+    cleanup();
+    return rc;
+  }
+  for (int sg = nck - 1; sg >= 0; sg--) {
+    const int x = sg & (nsets - 1), n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
+    CK(cudaStreamWaitEvent(sa, ev_rec[x], 0));
+    if (sg > 0) {
+      // set (sg-1) & 1 was read by the adjoint of segment sg+1
+      if (sg + 1 < nck) CK(cudaStreamWaitEvent(s, ev_adj[(sg - 1) & (nsets - 1)], 0));
+      if ((rc = replay(sg - 1)) != HARM_OK) {
+        cleanup();
+        return rc;
+      }
+    }
     for (int m = len - 1; m >= 0; m--) {
-      if (!w.adjg[m]) {
-        const Rec* r = &w.rec[m];
-        const double* po = w.pnext[m];
+      if (!w.adjg[x][m]) {
+        const Rec* r = &w.rec[x][m];
+        const double* po = w.pnext[x][m];
         AdjWork* wp = &w;
-        rc = capture_graph(c, [=](harm_ctx* t) {
+        rc = capture_graph(&ca, [=](harm_ctx* t) {
           adjoint_step(t, *wp, *r, po, w_mass, w_em);
           return HARM_OK;
-        }, &w.adjg[m]);
-        if (rc != HARM_OK) return rc;
+        }, &w.adjg[x][m]);
+        if (rc != HARM_OK) {
+          cleanup();
+          return rc;
+        }
       }
-      k_set_dt<<<1, 1, 0, s>>>(a, w.dts, n0 + m);
-      CK(cudaGraphLaunch(w.adjg[m], s));
+      k_set_dt<<<1, 1, 0, sa>>>(aa, w.dts, n0 + m);
+      CK(cudaGraphLaunch(w.adjg[x][m], sa));
     }
+    CK(cudaEventRecord(ev_adj[x], sa));
   }
   // through the input's bound: ghost adjoints onto the active zones
   {
     const dim3 b(32, 4);
-    k_adj_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, s>>>(a, w.La);
-    k_adj_ghosts<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, s>>>(a, w.La, in0.p);
+    k_adj_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, sa>>>(aa, w.La);
+    k_adj_ghosts<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, sa>>>(aa, w.La, in0.p);
   }
+  CK(cudaEventRecord(ev_join, sa));
+  CK(cudaStreamWaitEvent(s, ev_join, 0));
   CK(cudaEventRecord(e2, s));
   // the gradient in the reference layout
   {
@@ -1322,6 +1387,7 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
+  cleanup();
   return HARM_OK;
 }
 
