@@ -386,10 +386,15 @@ def b200_arm(a):
                                                           "on every SM, CUDA events"}
     for kname, per_zone in FP64_INSTR_PER_ZONE.items():
         if kname in prof and prof[kname][1]:
-            ms_l = prof[kname][0] / prof[kname][1]
+            # the k_update class times k_update with k_update_tail after it
+            # (two launches a substep): its per-launch time is per substep
+            nl = prof[kname][1] // 2 if kname == "k_update" else prof[kname][1]
+            ms_l = prof[kname][0] / nl
             rate = per_zone * n * n / (ms_l * 1e-3)
             fp64[kname] = {"fp64_instr_per_zone": per_zone, "achieved_per_s": rate, "launch_ms": ms_l,
                            "frac_of_dadd_peak": rate / fp64_rates["dadd"]}
+            if kname == "k_update":
+                fp64[kname]["launch_ms_includes"] = "k_update_tail"
     roofline["fp64"] = fp64
 
     mixed = None

@@ -36,7 +36,7 @@ __device__ __forceinline__ bool active(const StepArgs& a, int i, int j)
 }  // namespace
 
 // edot seed: d/dp of w dt (b^2 u^r u_t - b^r b_t) sqrt(-g) dx2 2pi at the
-// zones (0, j) of the step's final state (diag_flux's EM terms, as k_horizon
+// zones (0, j) of the step's final state (diag_flux's EM terms, as horizon_terms
 // forms); dt is the step's (a.sc->dt)
 __global__ void k_adj_seed_edot(StepArgs a, const double* __restrict__ pv, double* lam, double wfac)
 {

@@ -2,17 +2,23 @@
 //
 // Substep pipeline (reference step_ch.c:79-136 for one timeorder):
 //   k_flux         fluxcalc x1 and x2 faces + fix_flux + per-block dt minima
+//                  (with the flux switch, the first substep also forms the
+//                  b^2 flags and flux choices)
 //   k_emf          flux_ct corner EMFs (Toth, CORNGDETVERSION 1)
 //   k_update       advance_standard zone loop: U(pi), geometric source(pb),
 //                  flux divergence with the CT-rewritten B fluxes, RK combine,
 //                  2D Newton con-to-prim, fixup1zone
-//   k_bound        bound_prim + bound_pflag (ghost zones only)
-//   k_poledeath    the POLEDEATH zeroing of the first/last active x2 rows
-//   k_gammacheck,
+//   k_update_tail  inversions still unconverged after 16 Newton iterations
+//   k_bound_gc     bound_prim + bound_pflag (ghost zones) and the check-
+//                  solution gamma table
 //   k_checksol,
 //   k_checksol_rounds  fixup_checksolution (parallel fixed-point sweep, exact)
-//   k_fixup_*      fixup_utoprim from a snapshot
-//   k_bound/k_poledeath again, and k_dt_finalize after the last substep.
+//   k_fixup_compute    fixup_utoprim from a snapshot
+//   k_bound_fix    the repairs applied, the second bound and POLEDEATH; after
+//                  the last substep its last block also ends the step
+//                  (horizon sums, new dt)
+// The adjoint's recording path, the force-free step and the currents use
+// k_bound, k_poledeath, k_gammacheck, k_fixup_apply, k_bsqflags, k_step_end.
 #include <cuda_runtime.h>
 #include "harm_step_impl.cuh"
 #include "harm_tryagain.cuh"
