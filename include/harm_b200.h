@@ -286,8 +286,14 @@ void harm_ensemble_destroy(harm_ensemble* e);
    function theorem on its Jacobian, the conserved update and geometric
    source, flux-CT, the face fluxes (HLL/LAXF, wavespeeds, states) and the
    MC/PARA4 reconstructions differentiated piecewise, the repairs and the
-   boundary fills.  The context is left at p_N.  ms_out (may be NULL): the
-   forward and the backward wall times on the device.
+   boundary fills.  With more than one checkpoint segment the recomputation
+   of a segment runs on the context's stream while the adjoint of the
+   segment after it runs on a second stream (created and destroyed by the
+   call), from two record sets: device memory of about 2 x checkpoint_every
+   x 10 state-sized arrays (a 16-step segment of a 512^2 grid: ~3 GB a
+   set) besides one checkpoint per segment.  The context is left at p_N.
+   ms_out (may be NULL): the forward and the backward wall times on the
+   device.
 
    harm_run_fixed_dt: the same objective for nsteps steps with dt_n given
    (e.g. for finite differences against the adjoint). */
