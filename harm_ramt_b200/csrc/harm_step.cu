@@ -306,13 +306,14 @@ __global__ void k_bound(StepArgs a, double* pv, int with_pflag)
 // nothing changed them since), so the ghosts read the same value before or
 // after it is rewritten; a repaired one is read from the repair buffer.
 //
-// With step_end set (after the last substep) the grid carries extra rows of
-// blocks past the zones' (from block row `hrow0`): their threads form the
-// horizon terms of rows j from the final state of zone (0, j) -- the value
-// its own thread writes in this kernel: the repair buffer's or pv's, times
-// 0 for u~2 and B2 on the POLEDEATH rows (x * 0 of a value already zeroed
-// is the same zero) -- into ubuf, and the last block to finish runs
-// step_end_finish (the blocks count themselves in sc->blocks_done).
+// With step_end set (after the last substep) the grid starts with `hrows`
+// extra rows of blocks (launched first, so that their latency overlaps the
+// zones' work): their threads form the horizon terms of rows j from the
+// final state of zone (0, j) -- the value its own thread writes in this
+// kernel: the repair buffer's or pv's, times 0 for u~2 and B2 on the
+// POLEDEATH rows (x * 0 of a value already zeroed is the same zero) -- into
+// ubuf, and the last block to finish runs step_end_finish (the blocks count
+// themselves in sc->blocks_done).
 __device__ __forceinline__ void bound_fix_zone(const StepArgs& a, double* pv, int i, int j)
 {
   const int n1 = a.gr.n1, n2 = a.gr.n2;
@@ -337,13 +338,14 @@ __device__ __forceinline__ void bound_fix_zone(const StepArgs& a, double* pv, in
 }
 
 template <typename FT>
-__global__ void k_bound_fix(StepArgs a, double* pv, int step_end, int hrow0)
+__global__ void k_bound_fix(StepArgs a, double* pv, int step_end, int hrows)
 {
-  if ((int)blockIdx.y < hrow0) {
-    bound_fix_zone(a, pv, blockIdx.x * blockDim.x + threadIdx.x - NG, blockIdx.y * blockDim.y + threadIdx.y - NG);
+  if ((int)blockIdx.y >= hrows) {
+    bound_fix_zone(a, pv, blockIdx.x * blockDim.x + threadIdx.x - NG,
+                   (blockIdx.y - hrows) * blockDim.y + threadIdx.y - NG);
   } else {
     const int nt = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int j = ((blockIdx.y - hrow0) * gridDim.x + blockIdx.x) * nt + tid;
+    const int j = (blockIdx.y * gridDim.x + blockIdx.x) * nt + tid;
     if (j < a.gr.n2) {
       const long long pl = a.gr.plane, z = a.gr.at(0, j);
       double pr[NPR], t4[4];
@@ -375,10 +377,10 @@ __global__ void k_bound_fix(StepArgs a, double* pv, int step_end, int hrow0)
 
 void launch_bound_fix(int mixed, dim3 g, dim3 b, cudaStream_t s, const StepArgs& a, double* pv, int step_end)
 {
-  const int hrow0 = (int)g.y;
-  if (step_end) g.y += (a.gr.n2 + g.x * b.x * b.y - 1) / (g.x * b.x * b.y);
-  if (mixed) k_bound_fix<float><<<g, b, 0, s>>>(a, pv, step_end, hrow0);
-  else k_bound_fix<double><<<g, b, 0, s>>>(a, pv, step_end, hrow0);
+  const int hrows = step_end ? (a.gr.n2 + g.x * b.x * b.y - 1) / (g.x * b.x * b.y) : 0;
+  g.y += hrows;
+  if (mixed) k_bound_fix<float><<<g, b, 0, s>>>(a, pv, step_end, hrows);
+  else k_bound_fix<double><<<g, b, 0, s>>>(a, pv, step_end, hrows);
 }
 
 // POLEDEATH on the first and last active x2 rows (bounds.fishmon.c:296-327)

@@ -551,7 +551,7 @@ __device__ __forceinline__ void step_end_finish(const StepArgs& a, const double*
   constexpr int CHUNK = 256;
   __shared__ double sh[2][32];
   __shared__ double acc[4];
-  __shared__ double stage[4][CHUNK];
+  __shared__ double stage[4][CHUNK + 1];  // rows one double apart in banks: the four adding lanes do not conflict
   const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
   const int n2 = a.gr.n2;
   // chunks of the four term rows are staged in shared memory by the whole
@@ -560,6 +560,7 @@ __device__ __forceinline__ void step_end_finish(const StepArgs& a, const double*
   double s = 0.;
   for (int j0 = 0; j0 < n2; j0 += CHUNK) {
     const int m = (n2 - j0 < CHUNK) ? n2 - j0 : CHUNK;
+#pragma unroll 8
     for (int q = tid; q < 4 * m; q += nt) {
       const int k = q / m, jj = q - k * m;
       const double* src = t + k * ts + j0 + jj;
