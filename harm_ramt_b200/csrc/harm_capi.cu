@@ -1280,14 +1280,23 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   // set is replayed into only after the adjoint that read it has finished.
   cudaStream_t sa = nullptr;
   cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_adj[2] = {nullptr, nullptr}, ev_join = nullptr;
-  auto cleanup = [&]() {
-    for (int x = 0; x < 2; x++) {
-      if (ev_rec[x]) cudaEventDestroy(ev_rec[x]);
-      if (ev_adj[x]) cudaEventDestroy(ev_adj[x]);
+  // released on every return below (after the context's stream has drained
+  // what was enqueued on sa, or on an error path)
+  struct Release {
+    cudaStream_t& sa;
+    cudaEvent_t *ev_rec, *ev_adj;
+    cudaEvent_t& ev_join;
+    ~Release()
+    {
+      if (sa) cudaStreamSynchronize(sa);
+      for (int x = 0; x < 2; x++) {
+        if (ev_rec[x]) cudaEventDestroy(ev_rec[x]);
+        if (ev_adj[x]) cudaEventDestroy(ev_adj[x]);
+      }
+      if (ev_join) cudaEventDestroy(ev_join);
+      if (sa) cudaStreamDestroy(sa);
     }
-    if (ev_join) cudaEventDestroy(ev_join);
-    if (sa) cudaStreamDestroy(sa);
-  };
+  } release{sa, ev_rec, ev_adj, ev_join};
   CK(cudaStreamCreateWithFlags(&sa, cudaStreamNonBlocking));
   for (int x = 0; x < 2; x++) {
     CK(cudaEventCreateWithFlags(&ev_rec[x], cudaEventDisableTiming));
@@ -1322,20 +1331,14 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
     CK(cudaEventRecord(ev_rec[x], s));
     return HARM_OK;
   };
-  if ((rc = replay(nck - 1)) != HARM_OK) {
-    cleanup();
-    return rc;
-  }
+  if ((rc = replay(nck - 1)) != HARM_OK) return rc;
   for (int sg = nck - 1; sg >= 0; sg--) {
     const int x = sg & (nsets - 1), n0 = sg * checkpoint_every, len = std::min(checkpoint_every, nsteps - n0);
     CK(cudaStreamWaitEvent(sa, ev_rec[x], 0));
     if (sg > 0) {
       // set (sg-1) & 1 was read by the adjoint of segment sg+1
       if (sg + 1 < nck) CK(cudaStreamWaitEvent(s, ev_adj[(sg - 1) & (nsets - 1)], 0));
-      if ((rc = replay(sg - 1)) != HARM_OK) {
-        cleanup();
-        return rc;
-      }
+      if ((rc = replay(sg - 1)) != HARM_OK) return rc;
     }
     for (int m = len - 1; m >= 0; m--) {
       if (!w.adjg[x][m]) {
@@ -1346,10 +1349,7 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
           adjoint_step(t, *wp, *r, po, w_mass, w_em);
           return HARM_OK;
         }, &w.adjg[x][m]);
-        if (rc != HARM_OK) {
-          cleanup();
-          return rc;
-        }
+        if (rc != HARM_OK) return rc;
       }
       k_set_dt<<<1, 1, 0, sa>>>(aa, w.dts, n0 + m);
       CK(cudaGraphLaunch(w.adjg[x][m], sa));
@@ -1387,7 +1387,6 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
-  cleanup();
   return HARM_OK;
 }
 
