@@ -1297,7 +1297,14 @@ int harm_adjoint_run(harm_ctx* c, int nsteps, int checkpoint_every, double w_mas
       if (sa) cudaStreamDestroy(sa);
     }
   } release{sa, ev_rec, ev_adj, ev_join};
-  CK(cudaStreamCreateWithFlags(&sa, cudaStreamNonBlocking));
+  {
+    // the adjoint chain is the critical path (the replay only has to stay one
+    // segment ahead of it): its stream takes the device's highest priority,
+    // so that its blocks are scheduled first and the replay fills the rest
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CK(cudaStreamCreateWithPriority(&sa, cudaStreamNonBlocking, greatest));
+  }
   for (int x = 0; x < 2; x++) {
     CK(cudaEventCreateWithFlags(&ev_rec[x], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_adj[x], cudaEventDisableTiming));

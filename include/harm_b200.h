@@ -288,8 +288,9 @@ void harm_ensemble_destroy(harm_ensemble* e);
    MC/PARA4 reconstructions differentiated piecewise, the repairs and the
    boundary fills.  With more than one checkpoint segment the recomputation
    of a segment runs on the context's stream while the adjoint of the
-   segment after it runs on a second stream (created and destroyed by the
-   call), from two record sets: device memory of about 2 x checkpoint_every
+   segment after it runs on a second stream (created at the device's
+   highest stream priority and destroyed by the call), from two record
+   sets: device memory of about 2 x checkpoint_every
    x 10 state-sized arrays (a 16-step segment of a 512^2 grid: ~3 GB a
    set) besides one checkpoint per segment.  The context is left at p_N.
    ms_out (may be NULL): the forward and the backward wall times on the
