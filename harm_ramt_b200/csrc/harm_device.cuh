@@ -57,6 +57,11 @@ struct State {
   T ucon[4], ucov[4], bcon[4], bcov[4];
 };
 
+// v[d], d in 0..3, by selects: a constant d folds to v[d]; a run-time d
+// (one code path for both face directions) keeps v in registers
+template <typename T>
+HD_INLINE T pick4(const T* v, int d) { return (d == 3) ? v[3] : ((d == 2) ? v[2] : ((d == 1) ? v[1] : v[0])); }
+
 // gamma_calc, phys.c:848-877
 template <typename T>
 HD_INLINE T gamma_of(const T* pr, const Geo<T>& g)
@@ -123,8 +128,9 @@ HD_INLINE void mhd_row(const T* pr, int dir, const State<T>& q, T gam, T* mhd)
   T bsq = dot4(q.bcon, q.bcov);
   T eta = w + bsq;
   T ptot = P + bsq * T(0.5);
+  const T ud = pick4(q.ucon, dir), bd = pick4(q.bcon, dir);
 #pragma unroll
-  for (int j = 0; j < 4; j++) mhd[j] = eta * q.ucon[dir] * q.ucov[j] + ptot * ((dir == j) ? T(1.) : T(0.)) - q.bcon[dir] * q.bcov[j];
+  for (int j = 0; j < 4; j++) mhd[j] = eta * ud * q.ucov[j] + ptot * ((dir == j) ? T(1.) : T(0.)) - bd * q.bcov[j];
 }
 
 // primtoflux(UEVOLVE), phys.c:16-56, massflux_calc 59, dualfullfaraday_calc
@@ -133,12 +139,14 @@ template <typename T, bool FFDE>
 HD_INLINE void flux_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g, T gam, T* F)
 {
   T fin[NPR];
-  fin[RHO] = pr[RHO] * q.ucon[dir];
+  const T ud = pick4(q.ucon, dir);
+  fin[RHO] = pr[RHO] * ud;
   mhd_row<T, FFDE>(pr, dir, q, gam, &fin[UU]);
   if (dir > 0) {
-    fin[B1] = (pr[B1] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[1]) / q.ucon[0];
-    fin[B2] = (pr[B2] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[2]) / q.ucon[0];
-    fin[B3] = (pr[B3] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[3]) / q.ucon[0];
+    const T bd = pick4(&pr[B1 - 1], dir);  // B^dir
+    fin[B1] = (pr[B1] * ud - bd * q.ucon[1]) / q.ucon[0];
+    fin[B2] = (pr[B2] * ud - bd * q.ucon[2]) / q.ucon[0];
+    fin[B3] = (pr[B3] * ud - bd * q.ucon[3]) / q.ucon[0];
   } else {
     fin[B1] = pr[B1];
     fin[B2] = pr[B2];
@@ -179,7 +187,8 @@ HD_INLINE int vchar_of(const T* pr, const State<T>& q, int dir, const Geo<T>& g,
   T Acon[4], Bcon[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    Acon[m] = g.gcon[sym(m, dir)];
+    const T col[4] = {g.gcon[sym(m, 0)], g.gcon[sym(m, 1)], g.gcon[sym(m, 2)], g.gcon[sym(m, 3)]};
+    Acon[m] = pick4(col, dir);
     Bcon[m] = g.gcon[sym(m, 0)];
   }
   // dot(Acon,Acov) etc. with unit covectors: zero terms added exactly as the

@@ -51,8 +51,8 @@ __device__ __forceinline__ void face_flux(const StepArgs& a, int i, int j, int d
   if constexpr (sizeof(T) == 4) load_geo32(a, dir == 1 ? FACE1 : FACE2, z, g);
   else load_geo(a, dir == 1 ? FACE1 : FACE2, z, g);
   // B^dir continuity (BDIRCONT, step_ch.c:944-947)
-  const int bd = B1 + dir - 1;
-  p_l[bd] = p_r[bd] = T(0.5) * (p_l[bd] + p_r[bd]);
+  if (dir == 1) p_l[B1] = p_r[B1] = T(0.5) * (p_l[B1] + p_r[B1]);
+  else p_l[B2] = p_r[B2] = T(0.5) * (p_l[B2] + p_r[B2]);
   const T gmax = (T)a.pp.gammamax, gam = (T)a.pp.gam;
   int rc = limit_gamma(gmax, p_l, g);
   if (!rc) rc = limit_gamma(gmax, p_r, g);
@@ -139,10 +139,11 @@ __device__ __forceinline__ double block_min(double v, double* sh)
 // (blocks step by FLUX_BX = 31 along x1): lane 0 only lends its right state,
 // and its faces are the previous block's (block 0's lane 0 is zone -1,
 // which has no x1 face but an x2 face).
-// BY = 4 or 8 rows per block (flux_rows).  At most 128 registers a thread:
-// 512 threads per SM for the FP64 faces, four 4-row blocks for the FP32 ones.
+// BY = 4 or 8 rows per block (flux_rows).  At most 128 registers a thread
+// for the FP64 faces (512 threads per SM), 96 for the FP32 ones (five 4-row
+// blocks per SM).
 template <typename T, bool PARA, bool FFDE, int BY>
-__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 4 : 1))
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : ((BY == FLUX_BY_SMALL) ? 5 : 1))
     k_flux(StepArgs a, const __grid_constant__ CUtensorMap prim_map)
 {
   extern __shared__ __align__(128) double tile[];
@@ -208,42 +209,97 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 8) ? 512 / (32 * BY) : 
       rf = (int)a.fluxf[z];
     }
   }
-  // ---- x1 faces
-  zone_states<T, PARA>(tz, PS, 1, L, R);
+  if constexpr (sizeof(T) == 4) {
+    // FP32 faces (mixed form): both directions through one copy of the face
+    // code, dir a run-time value (the direction-dependent reads are
+    // selects), which halves the kernel's instruction footprint (the FP32
+    // kernel stalls on instruction fetch: 1% on the mixed step).  The FP64
+    // faces keep one copy per direction (below): the shared copy's register
+    // allocation cost them 0.3%.
+#pragma unroll 1
+    for (int dir = 1; dir <= 2; dir++) {
+      zone_states<T, PARA>(tz, PS, (dir == 1) ? 1 : FLUX_TILE_W, L, R);
+      bool act;
+      if (dir == 1) {
 #pragma unroll
-  for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
-  if (in && i >= 0 && tx > 0) {
-    face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij, rf);
-    dt1 = (dtij < dt1) ? dtij : dt1;
-    if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
-    if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
+        for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
+        act = in && i >= 0 && tx > 0;
+      } else {
 #pragma unroll
-    for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
-  }
-  // ---- x2 faces
-  zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
+        for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
+        __syncthreads();
+        if (ty > 0) {
 #pragma unroll
-  for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
-  __syncthreads();
-  if (ty > 0) {
+          for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
+        } else {
+          T Lm[NPR];
+          zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
+        }
+        act = in && j >= 0 && own;
+      }
+      if (act) {
+        face_flux<T, FFDE>(a, i, j, dir, pl, L, Fo, dtij, rf);
+        T* F;
+        if (dir == 1) {
+          // x1: fix_flux's mass-flux sign clamps at the two ends
+          dt1 = (dtij < dt1) ? dtij : dt1;
+          if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
+          if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
+          F = F1;
+        } else {
+          // x2: only u~2's flux crosses the polar and equatorial faces
+          dt2 = (dtij < dt2) ? dtij : dt2;
+          const bool polar = (j == 0 || j == n2) && (i < n1);
+          const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
+          if (polar || equator) {
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
-  } else {
-    T Lm[NPR];
-    zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
-  }
-  if (in && j >= 0 && own) {
-    face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij, rf);
-    dt2 = (dtij < dt2) ? dtij : dt2;
-    const bool polar = (j == 0 || j == n2) && (i < n1);
-    const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
-    if (polar || equator) {
+            for (int k = 0; k < NPR; k++)
+              if (k != U2) Fo[k] = T(0.);
+          }
+          F = F2;
+        }
 #pragma unroll
-      for (int k = 0; k < NPR; k++)
-        if (k != U2) Fo[k] = T(0.);
+        for (int k = 0; k < NPR; k++) F[k * a.gr.plane + z] = Fo[k];
+      }
     }
+  } else {
+    // ---- x1 faces
+    zone_states<T, PARA>(tz, PS, 1, L, R);
 #pragma unroll
-    for (int k = 0; k < NPR; k++) F2[k * a.gr.plane + z] = Fo[k];
+    for (int k = 0; k < NPR; k++) pl[k] = __shfl_up_sync(0xffffffffu, R[k], 1);
+    if (in && i >= 0 && tx > 0) {
+      face_flux<T, FFDE>(a, i, j, 1, pl, L, Fo, dtij, rf);
+      dt1 = (dtij < dt1) ? dtij : dt1;
+      if (i == 0 && a.pp.bc == 0 && j >= -1 && j < n2 && Fo[RHO] > 0) Fo[RHO] = 0;
+      if (i == n1 && j >= -1 && j < n2 && Fo[RHO] < 0) Fo[RHO] = 0;
+#pragma unroll
+      for (int k = 0; k < NPR; k++) F1[k * a.gr.plane + z] = Fo[k];
+    }
+    // ---- x2 faces
+    zone_states<T, PARA>(tz, PS, FLUX_TILE_W, L, R);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) shr[k][ty][tx] = R[k];
+    __syncthreads();
+    if (ty > 0) {
+#pragma unroll
+      for (int k = 0; k < NPR; k++) pl[k] = shr[k][ty - 1][tx];
+    } else {
+      T Lm[NPR];
+      zone_states<T, PARA>(tz - FLUX_TILE_W, PS, FLUX_TILE_W, Lm, pl);
+    }
+    if (in && j >= 0 && own) {
+      face_flux<T, FFDE>(a, i, j, 2, pl, L, Fo, dtij, rf);
+      dt2 = (dtij < dt2) ? dtij : dt2;
+      const bool polar = (j == 0 || j == n2) && (i < n1);
+      const bool equator = (j == (n2 - 1) / 2) && (i >= 0) && (i < n1);
+      if (polar || equator) {
+#pragma unroll
+        for (int k = 0; k < NPR; k++)
+          if (k != U2) Fo[k] = T(0.);
+      }
+#pragma unroll
+      for (int k = 0; k < NPR; k++) F2[k * a.gr.plane + z] = Fo[k];
+    }
   }
   dt1 = block_min(dt1, sh[0]);
   dt2 = block_min(dt2, sh[1]);
