@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--adjoint-ckpt", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=0,
                     help="if > 0, the adjoint leg runs this many steps instead of running to --adjoint-t")
+    ap.add_argument("--ffde-t", type=float, default=5.0,
+                    help="force-free leg (config C2, 512x256 dipole): both precisions run from init to this time "
+                         "(0: skip the leg)")
+    ap.add_argument("--ffde-steps", type=int, default=200, help="timed steps of the force-free leg")
     ap.add_argument("--sizes", default="512,1024",
                     help="grid sizes of the HLL/LAXF side measurements (empty: skip them)")
     ap.add_argument("--no-rows", action="store_true",
@@ -412,6 +416,7 @@ def b200_arm(a):
     sizes = None
     if a.sizes:
         sizes = sizes_leg(a, hb, stream, lim, barrier, dist)
+    ffde = ffde_leg(a, hb, stream, barrier, dist) if a.ffde_t > 0 else None
     window = same_window_leg(a, hb, stream, lim, flux, barrier, dist) if a.window_steps > 0 else None
     launches = sum(v[1] for v in prof.values()) * a.steps
     cpu = None
@@ -437,13 +442,64 @@ def b200_arm(a):
                            "state": f"torus advanced {a.evolve} steps from init (t={t_evolved:.4g}) before warm-up"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "mixed": mixed,
-                "ensemble": ens, "adjoint": adj, "rows": rows, "sizes": sizes, "same_window": window,
+                "ensemble": ens, "adjoint": adj, "rows": rows, "sizes": sizes, "ffde": ffde, "same_window": window,
                 "newton_iters_per_zone_substep": st["newton_iters"] / max(1, (a.evolve + a.warmup + a.steps + 1) * 2 * n * n),
                 "t_end": st["t"], "dt_end": st["dt"]}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def ffde_leg(a, hb, stream, barrier, dist):
+    """Config C2: the force-free aligned rotator (EOMFFDE on flat space,
+    defcoord 6 grid, r in [1, 100] stellar radii, dipole field, surface
+    rotating at 0.2; MC + LAXF), 512 x 256, built by the library's own
+    set-up.  FP64 and mixed each run from init to t = a.ffde_t (untimed),
+    then a.ffde_steps steps are timed with CUDA events.  Reported beside the
+    rates: the mixed state's relative L1 against FP64 at t = a.ffde_t (B and
+    the velocity), and the fraction of zones whose drift Lorentz factor sits
+    at the cap GAMMAMAX that enforces B^2 - E^2 > 0 (E.B = 0 holds by
+    construction of the inversion)."""
+    import torch
+    n1, n2, ng = 512, 256, hb.NG
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    out = {"workload": f"{n1}x{n2} force-free aligned rotator (flat space, log-r grid, r in [1, 100], dipole, "
+                       f"surface angular frequency 0.2), MC + LAXF, RK2, courant 0.8; state at t={a.ffde_t:g} "
+                       f"from init, then {a.ffde_steps} timed steps",
+           "data": "synthetic (init.ns.c dipole restated on the host: harm_dipole_geometry, harm_dipole_init)"}
+    at_t = {}
+    for name, prec in (("fp64", hb.PREC_FP64), ("mixed", hb.PREC_MIXED)):
+        h, g, _ = hb.dipole_context(n1, n2, precision=prec, stream=stream.cuda_stream)
+        st = h.run_to(a.ffde_t)
+        p, _ = h.get_prims()
+        at_t[name] = (p[ng:-ng, ng:-ng], st["realnstep"])
+        gc = g["gcov"][ng:-ng, ng:-ng, 3, 1:4, 1:4]
+        u = at_t[name][0][..., 2:5]
+        gamma = np.sqrt(1.0 + np.einsum("...i,...ij,...j->...", u, gc, u))
+        capped = float((gamma > 25.0 * (1 - 1e-9)).mean())
+        h.set_end_time(1.0e30)  # run_to left the end time at a.ffde_t: steps past it would have dt = 0
+        h.step_ch(a.warmup)
+        h.sync()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.step_ch(a.ffde_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / a.ffde_steps
+        prof = h.profile_step()
+        h.sync()
+        h.close()
+        out[name] = {"value": aggregate_rate(world, n1 * n2, ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                     "steps_to_t": int(at_t[name][1]), "zones_at_gamma_cap": capped,
+                     "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1]}}
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    pd, pm = at_t["fp64"][0], at_t["mixed"][0]
+    l1 = lambda x, y: float(np.abs(x - y).sum() / np.abs(y).sum())
+    out["mixed"]["l1_vs_fp64_at_t"] = {"B": l1(pm[..., 5:8], pd[..., 5:8]), "u": l1(pm[..., 2:5], pd[..., 2:5])}
+    return out
 
 
 def sizes_leg(a, hb, stream, lim, barrier, dist):

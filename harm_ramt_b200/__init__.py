@@ -92,6 +92,13 @@ class _TorusParams(ctypes.Structure):
                 ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double), ("gammamax", ctypes.c_double)]
 
 
+class _DipoleParams(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("rin", ctypes.c_double), ("rout", ctypes.c_double),
+                ("gam", ctypes.c_double), ("bpole", ctypes.c_double), ("omegastar", ctypes.c_double),
+                ("rhomin", ctypes.c_double), ("uumin", ctypes.c_double), ("rhominlimit", ctypes.c_double),
+                ("uuminlimit", ctypes.c_double), ("gammamax", ctypes.c_double)]
+
+
 _lib = None
 
 EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_prims", "harm_bound_prims",
@@ -101,7 +108,7 @@ EXPORTS = ["harm_create", "harm_upload_geometry", "harm_set_prims", "harm_get_pr
            "harm_torus_dump_coords", "harm_set_tiles", "harm_get_tiles", "harm_ensemble_create", "harm_ensemble_step",
            "harm_ensemble_sync", "harm_ensemble_destroy", "harm_adjoint_run", "harm_run_fixed_dt",
            "harm_torus_init_vpot", "harm_torus_vpot_to_field", "harm_torus_vpot_adjoint", "harm_invert_zones",
-           "harm_measure_fp64_peak"]
+           "harm_measure_fp64_peak", "harm_dipole_default_params", "harm_dipole_geometry", "harm_dipole_init"]
 
 
 def load_library(path=None):
@@ -156,6 +163,10 @@ def load_library(path=None):
     lib.harm_ensemble_destroy.argtypes = [vp]
     lib.harm_ensemble_destroy.restype = None
     lib.harm_torus_dump_coords.argtypes = [ctypes.POINTER(_TorusParams), ctypes.POINTER(_DumpHeader), dp]
+    lib.harm_dipole_default_params.argtypes = [ctypes.POINTER(_DipoleParams)]
+    lib.harm_dipole_default_params.restype = None
+    lib.harm_dipole_geometry.argtypes = [ctypes.POINTER(_DipoleParams), dp, dp, dp, dp, dp, dp]
+    lib.harm_dipole_init.argtypes = [ctypes.POINTER(_DipoleParams), dp, dp, dp, dp]
     lib.harm_measure_fp64_peak.argtypes = [dp]
     lib.harm_kernel_name.argtypes = [ctypes.c_int]
     lib.harm_kernel_name.restype = ctypes.c_char_p
@@ -510,6 +521,64 @@ def torus_dump_coords(params):
     co = np.zeros((params.n1 + 2 * NG, params.n2 + 2 * NG, 4))
     _check(lib.harm_torus_dump_coords(ctypes.byref(params), ctypes.byref(h), _dp(co)), "harm_torus_dump_coords")
     return {k: getattr(h, k) for k, _ in _DumpHeader._fields_}, co
+
+
+def dipole_params(n1=512, n2=256, **kw):
+    """The force-free aligned rotator's parameters (include/harm_setup.h)
+    with overrides."""
+    lib = load_library()
+    p = _DipoleParams()
+    lib.harm_dipole_default_params(ctypes.byref(p))
+    p.n1, p.n2 = n1, n2
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def dipole_geometry(params):
+    """set_grid() for the dipole grid (defcoord 6, flat space): dict of gcov,
+    gcon, gdet, conn, floors and the grid scalars (startx1, startx2, dx1,
+    dx2, Rin, Rout)."""
+    lib = load_library()
+    n1m, n2m = params.n1 + 2 * NG, params.n2 + 2 * NG
+    g = dict(gcov=np.zeros((n1m, n2m, 4, 4, 4)), gcon=np.zeros((n1m, n2m, 4, 4, 4)), gdet=np.zeros((n1m, n2m, 4)),
+             conn=np.zeros((n1m, n2m, 4, 4, 4)), floors=np.zeros((n1m, n2m, 2)))
+    grid = np.zeros(6)
+    _check(lib.harm_dipole_geometry(ctypes.byref(params), _dp(g["gcov"]), _dp(g["gcon"]), _dp(g["gdet"]),
+                                    _dp(g["conn"]), _dp(g["floors"]), _dp(grid)), "harm_dipole_geometry")
+    g.update(startx1=grid[0], startx2=grid[1], dx1=grid[2], dx2=grid[3], Rin=grid[4], Rout=grid[5])
+    return g
+
+
+def dipole_init(params, geom):
+    """init() for the dipole: every zone's primitives, ghosts included
+    (the state still to be bounded)."""
+    lib = load_library()
+    n1m, n2m = params.n1 + 2 * NG, params.n2 + 2 * NG
+    p = np.zeros((n1m, n2m, NPR))
+    _check(lib.harm_dipole_init(ctypes.byref(params), _dp(geom["gcov"]), _dp(geom["gcon"]), _dp(geom["gdet"]),
+                                _dp(p)), "harm_dipole_init")
+    return p
+
+
+def dipole_context(n1=512, n2=256, *, lim=LIM_MC, fluxmethod=FLUX_LAXF, cour=0.8, precision=PREC_FP64, tf=1.0e30,
+                   stream=None, currents=False, **dipole_kw):
+    """Builds the force-free aligned rotator on the host (MC + LAXF, the
+    reference's force-free defaults) and returns (HarmGPU, geometry, initial
+    prims) with the state uploaded, bounded and t=0, dt=1e-5 set."""
+    par = dipole_params(n1, n2, **dipole_kw)
+    geom = dipole_geometry(par)
+    p0 = dipole_init(par, geom)
+    h = HarmGPU(n1, n2, geom["dx1"], geom["dx2"], lim=lim, fluxmethod=fluxmethod, cour=cour, gam=par.gam,
+                gammamax=par.gammamax, precision=precision, tf=tf, stream=stream, eom=EOM_FFDE, bc=BC_STAR,
+                omegastar=par.omegastar, currents=currents)
+    h.upload_geometry(geom["gcov"], geom["gcon"], geom["gdet"], geom["conn"], geom["floors"])
+    h.set_prims(p0)
+    h.bound_prims()
+    h.set_time(0.0, 1.0e-5, 0)
+    return h, geom, p0
 
 
 def torus_context(n1=128, n2=128, *, lim=LIM_MC, fluxmethod=FLUX_HLL, cour=0.8, precision=PREC_FP64, tf=1.0e30,

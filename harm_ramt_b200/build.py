@@ -12,8 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libharm_b200.so")
 SOURCES = ["harm_capi.cu", "harm_step.cu", "harm_step_mixed.cu", "harm_adjoint.cu", "setup_torus.cpp",
-           "harm_fp64_peak.cu"]
-HEADERS = ["harm_device.cuh", "harm_kernels.cuh", "harm_step_impl.cuh", "harm_adjoint.cuh", "harm_tryagain.cuh", "harm_tma.cuh",
+           "setup_dipole.cu", "harm_fp64_peak.cu"]
+HEADERS = ["harm_device.cuh", "harm_kernels.cuh", "harm_step_impl.cuh", "harm_adjoint.cuh", "harm_tryagain.cuh", "harm_tma.cuh", "setup_grid.h",
            "../../include/harm_b200.h", "../../include/harm_setup.h"]
 
 COMMON = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]

@@ -574,7 +574,9 @@ int harm_bound_prims(harm_ctx* c)
   const StepArgs a = c->args();
   const dim3 b(32, 4);
   k_bound<<<grid2(c->cfg.n1 + 2 * NG, c->cfg.n2 + 2 * NG, b), b, 0, c->stream>>>(a, c->d_p, 1);
-  k_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, c->stream>>>(a, c->d_p);
+  // POLEDEATH belongs to the torus's bound (bounds.fishmon.c); the star's
+  // (bounds.ns.c) keeps the first and last rows as they are
+  if (c->cfg.bc == HARM_BC_TORUS) k_poledeath<<<dim3((c->cfg.n1 + 127) / 128, 2), 128, 0, c->stream>>>(a, c->d_p);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return HARM_OK;

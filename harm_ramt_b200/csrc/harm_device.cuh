@@ -438,12 +438,11 @@ HD_INLINE int ucon_3vel(const double* v, const double* c, double* ucon)
 // B^2 - E^2 > 0 cap on the drift Lorentz factor, v^i (EBcovtovcon,
 // 551-560), u^i through ucon_calc_3vel (vcon2pr's active branch,
 // transforms.c:372-377, stores u^i).  pr[RHO], pr[UU] keep the guess.
-// Returns 0 or FAIL_FFDE_SPACELIKE.
-HD_INLINE int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, double gammamax)
+// Returns 0 or FAIL_FFDE_SPACELIKE.  utoprim_ffde_geomfree takes U in the
+// geometry-free form (T^t_mu, B^i), as filterffde (phys.ffde.c:1957-1980)
+// passes it; utoprim_ffde the evolved form (times sqrt(-g)).
+HD_INLINE int utoprim_ffde_geomfree(const double* U, const Geo<double>& g, double* pr, double gammamax)
 {
-  double U[NPR];
-#pragma unroll
-  for (int k = 0; k < NPR; k++) U[k] = Uin[k] / g.g;
   const double alphasq = 1. / (-g.gcon[0]);
   double Bcon[4] = {0.0, U[B1], U[B2], U[B3]}, Bcov[4];
   lower_v(Bcon, g.gcov, Bcov);
@@ -482,6 +481,14 @@ HD_INLINE int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, 
   pr[B2] = U[B2];
   pr[B3] = U[B3];
   return 0;
+}
+
+HD_INLINE int utoprim_ffde(const double* Uin, const Geo<double>& g, double* pr, double gammamax)
+{
+  double U[NPR];
+#pragma unroll
+  for (int k = 0; k < NPR; k++) U[k] = Uin[k] / g.g;
+  return utoprim_ffde_geomfree(U, g, pr, gammamax);
 }
 
 // lower_g / raise_g of utoprim_2d.c:365-392: sums started from 0.

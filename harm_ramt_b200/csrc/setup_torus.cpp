@@ -16,282 +16,11 @@
 
 #include "../../include/harm_b200.h"
 #include "../../include/harm_setup.h"
+#include "setup_grid.h"
 
 namespace {
 
-constexpr int NG = 3;
-constexpr int FACE1 = 0, FACE2 = 1, CORN = 2, CENT = 3;
-enum { RHO = 0, UU, U1, U2, U3, B1, B2, B3 };
-
-struct Coords {
-  double a, R0, Rin, Rout, hslope, startx1, startx2, dx1, dx2;
-};
-
-// coord(), coord.c:920-938
-void coord_of(const Coords& c, int i, int j, int loc, double* X)
-{
-  if (loc == FACE1) {
-    X[1] = c.startx1 + (i + 0) * c.dx1;
-    X[2] = c.startx2 + ((j + 0) + 0.5) * c.dx2;
-  } else if (loc == FACE2) {
-    X[1] = c.startx1 + ((i + 0) + 0.5) * c.dx1;
-    X[2] = c.startx2 + (j + 0) * c.dx2;
-  } else if (loc == CENT) {
-    X[1] = c.startx1 + ((i + 0) + 0.5) * c.dx1;
-    X[2] = c.startx2 + ((j + 0) + 0.5) * c.dx2;
-  } else {
-    X[1] = c.startx1 + (i + 0) * c.dx1;
-    X[2] = c.startx2 + (j + 0) * c.dx2;
-  }
-  X[0] = X[3] = 0.0;
-}
-
-// bl_coord for defcoord 0 with COORDSINGFIX, coord.c:334-453
-void bl_of(const Coords& c, const double* X, double* r, double* th)
-{
-  *r = c.R0 + exp(X[1]);
-  *th = M_PI * X[2] + ((1. - c.hslope) / 2.) * sin(2. * M_PI * X[2]);
-  if (fabs(*th) < 1E-20) {
-    if (*th >= 0) *th = 1E-20;
-    if (*th < 0) *th = -1E-20;
-  }
-}
-
-// dxdxp_analytic defcoord 0 (diagonal), coord.c:480-491
-void dxdxp_of(const Coords& c, const double* X, double r, double d[4])
-{
-  d[0] = 1.0;
-  d[1] = r - c.R0;
-  d[2] = M_PI + (1. - c.hslope) * M_PI * cos(2. * M_PI * X[2]);
-  d[3] = 1.0;
-}
-
-// set_gcov_ksmetric (metric.c:540-597) then gcov2gcovprim (metric.c:1057-1083)
-// with the diagonal Jacobian: g'_{jk} = (g_{jk} d_j) d_k
-void gcov_prim(const Coords& c, const double* X, double g[4][4])
-{
-  double r, th;
-  bl_of(c, X, &r, &th);
-  const double a = c.a;
-  const double cth = cos(th), sth = sin(th), s2 = sth * sth;
-  const double rho2 = r * r + a * a * cth * cth;
-  double ks[4][4];
-  ks[0][0] = (-1. + 2. * r / rho2);
-  ks[0][1] = (2. * r / rho2);
-  ks[0][2] = (0);
-  ks[0][3] = (-2. * a * r * s2 / rho2);
-  ks[1][0] = ks[0][1];
-  ks[1][1] = (1. + 2. * r / rho2);
-  ks[1][2] = (0);
-  ks[1][3] = (-a * s2 * (1. + 2. * r / rho2));
-  ks[2][0] = (0);
-  ks[2][1] = (0);
-  ks[2][2] = (rho2);
-  ks[2][3] = (0);
-  ks[3][0] = ks[0][3];
-  ks[3][1] = ks[1][3];
-  ks[3][2] = (0);
-  ks[3][3] = (s2 * (rho2 + a * a * s2 * (1. + 2. * r / rho2)));
-  double d[4];
-  dxdxp_of(c, X, r, d);
-  double dm[4][4] = {{0}};
-  for (int k = 0; k < 4; k++) dm[k][k] = d[k];
-  for (int j = 0; j < 4; j++)
-    for (int k = 0; k < 4; k++) {
-      double t = 0.;
-      for (int l = 0; l < 4; l++)
-        for (int m = 0; m < 4; m++) t += ks[l][m] * dm[l][j] * dm[m][k];
-      g[j][k] = t;
-    }
-}
-
-// set_gcon_ksmetric (metric.c:666-722) then gcon2gconprim (metric.c:1085-1106);
-// the inverse Jacobian of a diagonal matrix is its reciprocal diagonal
-// (which the reference's Gauss-Jordan produces exactly: pivot 1/d_kk).
-void gcon_prim(const Coords& c, const double* X, double g[4][4])
-{
-  double r, th;
-  bl_of(c, X, &r, &th);
-  const double a = c.a;
-  const double cth = cos(th), sth = sin(th), s2 = sth * sth;
-  const double rho2 = r * r + a * a * cth * cth;
-  double ks[4][4];
-  ks[0][0] = (-(1. + 2. * r / rho2));
-  ks[0][1] = (2. * r / rho2);
-  ks[0][2] = (0);
-  ks[0][3] = (0);
-  ks[1][0] = ks[0][1];
-  ks[1][1] = ((r * (r - 2.) + a * a) / rho2);
-  ks[1][2] = (0);
-  ks[1][3] = (a / rho2);
-  ks[2][0] = ks[0][2];
-  ks[2][1] = ks[1][2];
-  ks[2][2] = (1. / rho2);
-  ks[2][3] = (0);
-  ks[3][0] = ks[0][3];
-  ks[3][1] = ks[1][3];
-  ks[3][2] = ks[2][3];
-  ks[3][3] = (1. / (rho2 * s2));
-  double d[4];
-  dxdxp_of(c, X, r, d);
-  double id[4][4] = {{0}};
-  for (int k = 0; k < 4; k++) id[k][k] = 1.0 / d[k];
-  for (int j = 0; j < 4; j++)
-    for (int k = 0; k < 4; k++) {
-      double t = 0.;
-      for (int l = 0; l < 4; l++)
-        for (int m = 0; m < 4; m++) t += id[j][l] * id[k][m] * ks[l][m];
-      g[j][k] = t;
-    }
-}
-
-// gdet_func, metric.c:1109-1140: LU decomposition with implicit partial
-// pivoting (the Numerical Recipes ludcmp of ludcmp.c), det = d * prod(diag)
-double gdet_of(const double gin[4][4])
-{
-  double a[5][5], vv[5], d = 1.0;
-  for (int j = 0; j < 4; j++)
-    for (int k = 0; k < 4; k++) a[j + 1][k + 1] = gin[j][k];
-  const int n = 4;
-  int imax = 0;
-  for (int i = 1; i <= n; i++) {
-    double big = 0.0, temp;
-    for (int j = 1; j <= n; j++)
-      if ((temp = fabs(a[i][j])) > big) big = temp;
-    if (big == 0.0) return NAN;
-    vv[i] = 1.0 / big;
-  }
-  for (int j = 1; j <= n; j++) {
-    for (int i = 1; i < j; i++) {
-      double sum = a[i][j];
-      for (int k = 1; k < i; k++) sum -= a[i][k] * a[k][j];
-      a[i][j] = sum;
-    }
-    double big = 0.0, dum;
-    for (int i = j; i <= n; i++) {
-      double sum = a[i][j];
-      for (int k = 1; k < j; k++) sum -= a[i][k] * a[k][j];
-      a[i][j] = sum;
-      if ((dum = vv[i] * fabs(sum)) >= big) {
-        big = dum;
-        imax = i;
-      }
-    }
-    if (j != imax) {
-      for (int k = 1; k <= n; k++) {
-        dum = a[imax][k];
-        a[imax][k] = a[j][k];
-        a[j][k] = dum;
-      }
-      d = -d;
-      vv[imax] = vv[j];
-    }
-    if (a[j][j] == 0.0) a[j][j] = 1.0e-30;
-    if (j != n) {
-      dum = 1.0 / (a[j][j]);
-      for (int i = j + 1; i <= n; i++) a[i][j] *= dum;
-    }
-  }
-  for (int j = 1; j <= n; j++) d *= a[j][j];
-  return (d >= 0) ? NAN : sqrt(-d);
-}
-
-// conn_func_numerical1 with GAMMIEDERIVATIVE and CONNDELTA 1e-5,
-// metric.c:1188-1262: centred differences of g'_{mu nu}, lowered Christoffel
-// symbols, then raised with g'^{mu nu} at CENT.  conn[k][l][j] = Gamma^k_{lj}.
-void conn_of(const Coords& c, const double* X, const double gcon[4][4], double conn[4][4][4])
-{
-  const double DELTA = 1E-5;
-  double dg[4][4][4], tmp[4][4][4];
-  for (int k = 0; k < 4; k++) {
-    double Xh[4], Xl[4], gh[4][4], gl[4][4];
-    for (int l = 0; l < 4; l++) Xh[l] = Xl[l] = X[l];
-    Xh[k] += DELTA;
-    Xl[k] -= DELTA;
-    gcov_prim(c, Xh, gh);
-    gcov_prim(c, Xl, gl);
-    for (int i = 0; i < 4; i++)
-      for (int j = 0; j < 4; j++) dg[i][j][k] = (gh[i][j] - gl[i][j]) / (Xh[k] - Xl[k]);
-  }
-  for (int i = 0; i < 4; i++)
-    for (int j = 0; j < 4; j++)
-      for (int k = 0; k < 4; k++) tmp[i][j][k] = 0.5 * (dg[j][i][k] + dg[k][i][j] - dg[k][j][i]);
-  for (int i = 0; i < 4; i++)
-    for (int j = 0; j < 4; j++)
-      for (int k = 0; k < 4; k++) {
-        double s = 0.;
-        for (int l = 0; l < 4; l++) s += gcon[i][l] * tmp[l][j][k];
-        conn[i][j][k] = s;
-      }
-}
-
-// ------------------------------------------------------------------ state
-struct G {
-  const double* gcov;  // 16
-  const double* gcon;  // 16
-  double g;
-};
-
-double gamma_of(const double* pr, const G& g)
-{
-  const double* c = g.gcov;
-  double qsq = c[5] * pr[U1] * pr[U1] + c[10] * pr[U2] * pr[U2] + c[15] * pr[U3] * pr[U3] +
-               2. * (c[6] * pr[U1] * pr[U2] + c[7] * pr[U1] * pr[U3] + c[11] * pr[U2] * pr[U3]);
-  return sqrt(1. + qsq);
-}
-
-void ucon_rel4(const double* pr, const G& g, double* ucon)
-{
-  double alpha = 1. / sqrt(-g.gcon[0]);
-  double b1 = g.gcon[1] * alpha * alpha, b2 = g.gcon[2] * alpha * alpha, b3 = g.gcon[3] * alpha * alpha;
-  double gamma = gamma_of(pr, g);
-  ucon[0] = gamma / alpha;
-  ucon[1] = pr[U1] - gamma * b1 / alpha;
-  ucon[2] = pr[U2] - gamma * b2 / alpha;
-  ucon[3] = pr[U3] - gamma * b3 / alpha;
-}
-
-void lower4(const double* v, const double* c, double* w)
-{
-  w[0] = c[0] * v[0] + c[1] * v[1] + c[2] * v[2] + c[3] * v[3];
-  w[1] = c[1] * v[0] + c[5] * v[1] + c[6] * v[2] + c[7] * v[3];
-  w[2] = c[2] * v[0] + c[6] * v[1] + c[10] * v[2] + c[11] * v[3];
-  w[3] = c[3] * v[0] + c[7] * v[1] + c[11] * v[2] + c[15] * v[3];
-}
-
-double bsq_of(const double* pr, const G& g)
-{
-  double ucon[4], ucov[4], bcon[4], bcov[4];
-  ucon_rel4(pr, g, ucon);
-  lower4(ucon, g.gcov, ucov);
-  bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
-  for (int j = 1; j <= 3; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[0] * ucon[j]) / ucon[0];
-  lower4(bcon, g.gcov, bcov);
-  return bcon[0] * bcov[0] + bcon[1] * bcov[1] + bcon[2] * bcov[2] + bcon[3] * bcov[3];
-}
-
-// ucon2pr(VELREL4), transforms.c:322-346
-void ucon_to_rel4(const double* ucon, const G& g, double* pr)
-{
-  double alphasq = 1. / (-g.gcon[0]);
-  double gammaoalpha = ucon[0];
-  for (int j = 1; j <= 3; j++) pr[U1 + j - 1] = ucon[j] + alphasq * g.gcon[j] * gammaoalpha;
-}
-
-int limit_gamma(double gammamax, double* pr, const G& g)
-{
-  if (gammamax <= 1.0) return 0;
-  double gamma = gamma_of(pr, g);
-  if (gamma > gammamax && gamma != 1.0) {
-    double pref = (gammamax * gammamax - 1.) / (gamma * gamma - 1.);
-    if (pref < 0.0) return 1;
-    double f = sqrt(pref);
-    pr[U1] *= f;
-    pr[U2] *= f;
-    pr[U3] *= f;
-  }
-  return 0;
-}
+using namespace harm_setup;
 
 // the reference's seeded generator ranc() (ranc.c:31-54) over libc rand()
 struct Ranc {
@@ -355,7 +84,7 @@ int harm_torus_geometry(const harm_torus_params* P, double* gcov, double* gcon, 
                         double* grid_out)
 {
   if (!P || !gcov || !gcon || !gdet || !conn || !floors) return HARM_EINVAL;
-  const int n1 = P->n1, n2 = P->n2, n1m = n1 + 2 * NG, n2m = n2 + 2 * NG;
+  const int n1 = P->n1, n2 = P->n2;
   Coords c;
   c.a = P->a;
   c.R0 = 0.0;
@@ -368,32 +97,8 @@ int harm_torus_geometry(const harm_torus_params* P, double* gcov, double* gcon, 
   c.startx2 = 0.;
   c.dx1 = log((c.Rout - c.R0) / (c.Rin - c.R0)) / n1;
   c.dx2 = 1. / n2;
-  for (int i = -NG; i < n1 + NG; i++)
-    for (int j = -NG; j < n2 + NG; j++) {
-      const long long zr = (long long)(i + NG) * n2m + (j + NG);
-      for (int loc = 3; loc >= 0; loc--) {
-        double X[4], gv[4][4], gn[4][4];
-        coord_of(c, i, j, loc, X);
-        gcov_prim(c, X, gv);
-        gcon_prim(c, X, gn);
-        memcpy(gcov + (zr * 4 + loc) * 16, gv, sizeof(gv));
-        memcpy(gcon + (zr * 4 + loc) * 16, gn, sizeof(gn));
-        gdet[zr * 4 + loc] = gdet_of(gv);
-        if (loc == CENT) {
-          double cn[4][4][4];
-          conn_of(c, X, gn, cn);
-          memcpy(conn + zr * 64, cn, sizeof(cn));
-          // set_density_floors rescaletype 0 + fixup1zone clamps, fixup.c:996-1110, 295-307
-          double r, th;
-          bl_of(c, X, &r, &th);
-          double fr = P->rhomin * pow(r, -1.5), fu = P->uumin * pow(r, -2.5);
-          if (fr < P->rhominlimit) fr = P->rhominlimit;
-          if (fu < P->uuminlimit) fu = P->uuminlimit;
-          floors[zr * 2 + 0] = fr;
-          floors[zr * 2 + 1] = fu;
-        }
-      }
-    }
+  if (grid_tables(c, n1, n2, P->rhomin, P->uumin, P->rhominlimit, P->uuminlimit, gcov, gcon, gdet, conn, floors))
+    return HARM_EINVAL;
   if (grid_out) {
     grid_out[0] = c.startx1;
     grid_out[1] = c.startx2;
@@ -402,7 +107,6 @@ int harm_torus_geometry(const harm_torus_params* P, double* gcov, double* gcon, 
     grid_out[4] = c.Rin;
     grid_out[5] = rhor;
   }
-  (void)n1m;
   return HARM_OK;
 }
 

@@ -157,7 +157,9 @@ int harm_set_prims(harm_ctx* ctx, const double* prims, const int* pflag, int res
 int harm_get_prims(harm_ctx* ctx, double* prims, int* pflag);
 
 /* Fills the ghost zones of the device state as bound_prim() does
-   (bounds.fishmon.c:14-330), e.g. after uploading an unbounded state. */
+   (bounds.fishmon.c:14-330 with the torus's POLEDEATH zeroing of the first
+   and last active rows, or bounds.ns.c:10-355 for HARM_BC_STAR), e.g. after
+   uploading an unbounded state. */
 int harm_bound_prims(harm_ctx* ctx);
 
 /* Sets t, dt and realnstep (as init() or a restart leaves them). */

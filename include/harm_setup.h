@@ -1,7 +1,8 @@
 /*
  * harm_setup.h -- host-side problem set-up for standalone runs: the grid
- * geometry and the Fishbone-Moncrief torus of the reference's plugin
- * surface (coord.c, metric.c, set_grid.c, init.fishmon.c, initbase.c).
+ * geometry and the initial state of the reference's plugin surface (coord.c,
+ * metric.c, set_grid.c, initbase.c) for the Fishbone-Moncrief torus
+ * (init.fishmon.c) and the force-free aligned rotator (init.ns.c).
  *
  * A drop-in host keeps calling the reference's own set_grid()/init(); these
  * entry points exist so that the library can produce the same inputs without
@@ -76,6 +77,45 @@ int harm_torus_vpot_adjoint(const harm_torus_params* p, const double* gdet, cons
    header's plugin scalars (defcoord 0) and X1, X2, r, th at every zone
    centre, [n1m][n2m][4] (coord.c:920-938, bl_coord coord.c:334-453). */
 int harm_torus_dump_coords(const harm_torus_params* p, harm_dump_header* hdr, double* coords);
+
+/* The force-free aligned rotator of init.ns.c + bounds.ns.c (EOMFFDE,
+   MCOORD SPCMINKMETRIC): flat space in spherical polar coordinates,
+   defcoord 6 (log r, uniform theta), r in [rin, rout] stellar radii, a dipole
+   field A_phi = bpole rin^3 sin^2(theta) / (2 r) (init.ns.c:525) and a
+   stellar surface rotating at omegastar (bounds.ns.c:108). */
+typedef struct harm_dipole_params {
+  int n1, n2;             /* interior zones */
+  double rin, rout;       /* stellar surface and outer radius (init_grid) */
+  double gam;             /* adiabatic index (init_global) */
+  double bpole;           /* polar field (pre_init_specific_init, init.ns.c:50) */
+  double omegastar;       /* surface angular frequency (HARM_BC_STAR) */
+  double rhomin, uumin;   /* floor coefficients (init_global, rescaletype 0) */
+  double rhominlimit, uuminlimit;
+  double gammamax;
+} harm_dipole_params;
+
+/* 512 x 256, rin 1, rout 100, gamma 4/3, bpole 1, omegastar 0.2, floors
+   1e-10 r^-1.5 / 1e-11 r^-2.5, GAMMAMAX 25. */
+void harm_dipole_default_params(harm_dipole_params* p);
+
+/* set_grid() for defcoord 6 on flat space (the metric inverse by
+   Gauss-Jordan, matrix_inverse, metric.c:1146-1162): the tables of
+   harm_torus_geometry() for the dipole grid.  grid_out (may be NULL)
+   receives startx1, startx2, dx1, dx2, Rin, Rout. */
+int harm_dipole_geometry(const harm_dipole_params* p, double* gcov, double* gcon, double* gdet, double* conn,
+                         double* floors, double* grid_out);
+
+/* init()'s fresh start (initbase.c:297-562) for EOMFFDE with init.ns.c's
+   star without a disk: the zero atmosphere (set_atmosphere, fixup.c:1119-1190)
+   round-tripped through the relative 4-velocity, the dipole vector potential
+   at every corner and vpot2field over the whole grid (initbase.c:565-618),
+   filterffde twice (phys.ffde.c:1957-1980: state, conserved quantities and
+   the force-free inversion, densities zeroed), then fixup's Lorentz-factor
+   limit on the active zones.  Every zone is set, ghost zones included (the
+   star's boundary holds the ghosts' field); the caller still bounds the
+   state (harm_bound_prims() on the device). */
+int harm_dipole_init(const harm_dipole_params* p, const double* gcov, const double* gcon, const double* gdet,
+                     double* prims);
 
 #ifdef __cplusplus
 }
