@@ -494,6 +494,7 @@ def ffde_leg(a, hb, stream, barrier, dist):
         h.close()
         out[name] = {"value": aggregate_rate(world, n1 * n2, ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
                      "steps_to_t": int(at_t[name][1]), "zones_at_gamma_cap": capped,
+                     "max_drift_gamma": float(gamma.max()),
                      "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1]}}
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     pd, pm = at_t["fp64"][0], at_t["mixed"][0]
